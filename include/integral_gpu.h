@@ -1,0 +1,163 @@
+/*
+ * integral_gpu.h — C ABI of the B200 (sm_100a) two-electron integral path.
+ *
+ * Drop-in boundary for the Rust crate `integral` (nmrtist/integral 0.4.3):
+ * the crate's C-ABI crate `integral-sys` exports only
+ * `integral_abi_version()` (crates/integral-sys/src/lib.rs:21); the entry
+ * points below extend that seam with the GPU-backed two-electron path so the
+ * Rust host (Basis, EriBuilder, DirectContractor, DirectGradContractor) can
+ * call CUDA through plain pointers and sizes.  Every entry point returns an
+ * int status (IGPU_OK = 0, negative = error, never unwinds); the message of
+ * the last failure on the calling thread is igpu_last_error_string().
+ *
+ * Layouts follow the reference exactly:
+ *   - AO order = shell order, n_func per shell (Cartesian (l+1)(l+2)/2 in
+ *     src/math/am.rs order, spherical 2l+1 in solid_harmonics::m_order order);
+ *   - dense ERI: eri[((i*nao + j)*nao + k)*nao + l] (src/integrals.rs:646-654);
+ *   - densities / J / K: row-major nao x nao, ndens of them back to back;
+ *   - gradient: dE/dR (not force), natom x 3, atoms in Basis::atoms() order
+ *     (first appearance of a bitwise-equal centre, src/shell.rs:250-258).
+ * Outputs of igpu_jk*, igpu_grad* ACCUMULATE (+=) into the caller's buffers
+ * (src/direct.rs:398-403, src/direct_grad.rs:476-484); igpu_eri_dense and
+ * igpu_eri_builder_fill ASSIGN.
+ */
+#ifndef INTEGRAL_GPU_H
+#define INTEGRAL_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IGPU_ABI_VERSION 1u
+
+/* status codes (IntegralError variants of src/lib.rs:83-118 plus the
+ * misuse panics of src/direct.rs:141-159 / src/direct_grad.rs:337-346) */
+#define IGPU_OK 0
+#define IGPU_ERR_INVALID_ARGUMENT (-1)
+#define IGPU_ERR_EMPTY_CONTRACTION (-2)       /* IntegralError::EmptyContraction */
+#define IGPU_ERR_MISMATCHED_CONTRACTION (-3)  /* IntegralError::MismatchedContraction */
+#define IGPU_ERR_ANGULAR_MOMENTUM (-4)        /* IntegralError::AngularMomentumTooHigh */
+#define IGPU_ERR_ANGULAR_MOMENTUM_GRAD (-5)   /* ...TooHighForGradient */
+#define IGPU_ERR_DENSITY_COUNT (-6)           /* 1..64 densities (direct.rs:141-148) */
+#define IGPU_ERR_LENGTH (-7)                  /* buffer length mismatch */
+#define IGPU_ERR_NONCANONICAL_BRA (-8)        /* bra pair index out of range */
+#define IGPU_ERR_CUDA (-9)
+#define IGPU_ERR_OUT_OF_MEMORY (-10)
+#define IGPU_ERR_UNSUPPORTED (-11)            /* class not built for the GPU */
+#define IGPU_ERR_NO_DEVICE (-12)
+
+/* Engine (src/integrals.rs:329-338).  The GPU evaluates every quartet by Rys
+ * quadrature; the value is kept so the plan reports what the host asked for. */
+#define IGPU_ENGINE_AUTO 0
+#define IGPU_ENGINE_OSHGP 1
+#define IGPU_ENGINE_RYS 2
+
+/* Arithmetic of the quartet kernels.  FP64: every quartet in double.
+ * MIXED: quartets whose Schwarz estimate Q_ij*Q_kl*max|D| is below the
+ * plan's cutoff run their Rys roots, recurrences and contraction in FP32,
+ * the rest in FP64; all J/K/gradient accumulation is FP64. */
+#define IGPU_PRECISION_FP64 0
+#define IGPU_PRECISION_MIXED 1
+
+typedef struct igpu_plan igpu_plan;
+
+/* One contracted shell (src/shell.rs:49-55): raw contraction coefficients;
+ * the plan applies the per-primitive normalisation (shell.rs:182-187). */
+typedef struct {
+  int l;
+  int spherical; /* 0 Cartesian, 1 real spherical */
+  double center[3];
+  int nprim;
+  const double* exps;
+  const double* coefs;
+} igpu_shell;
+
+/* One product term factor * left (x) right of a two-particle density
+ * (GradDensityTerm, src/direct_grad.rs:21-25); left/right symmetric nao x nao. */
+typedef struct {
+  double factor;
+  const double* left;
+  const double* right;
+} igpu_term;
+
+/* Counters of the last J/K or gradient call on a plan. */
+typedef struct {
+  uint64_t quartets;          /* canonical shell quartets that survived screening */
+  uint64_t quartet_hash;      /* order-independent fingerprint of that list */
+  uint64_t quartets_fp32;     /* of them, evaluated in FP32 (MIXED) */
+  uint64_t prim_quartets;     /* surviving primitive quartets */
+  double model_flops;         /* fixed Rys flop model of the surviving work */
+  double kernel_ms;           /* device time of the quartet kernels */
+  uint32_t launches;          /* kernels launched by the call */
+} igpu_stats;
+
+/* integral-sys `integral_abi_version` (crates/integral-sys/src/lib.rs:21). */
+uint32_t igpu_abi_version(void);
+
+const char* igpu_last_error_string(void);
+
+/* Plan = DirectContractor::with_engine / DirectGradContractor::with_engine /
+ * EriBuilder::with_engine precompute (src/direct.rs:59-87,
+ * src/direct_grad.rs:180-247, src/eri_builder.rs:238-270): shells, offsets,
+ * effective coefficients, c2s, canonical pairs, primitive-pair data and the
+ * Schwarz bounds (computed on the device once, at creation). */
+int igpu_plan_create(const igpu_shell* shells, size_t nsh, int engine, igpu_plan** out);
+int igpu_plan_destroy(igpu_plan* plan);
+/* Basis::nao (shell.rs:160), Basis::atoms().len(), bra_pairs().len(), nsh. */
+int igpu_plan_query(const igpu_plan* plan, size_t* nao, size_t* natom, size_t* nbra, size_t* nsh);
+/* DirectContractor::bra_pairs (direct.rs:95): canonical (i, j), i >= j,
+ * row-major; pairs[2p] = i, pairs[2p+1] = j. */
+int igpu_bra_pairs(const igpu_plan* plan, uint32_t* pairs);
+/* Basis::atoms (shell.rs:250-258): natom x 3 centres. */
+int igpu_atoms(const igpu_plan* plan, double* xyz);
+/* Basis::schwarz_bounds (integrals.rs:835-862): nsh x nsh, row-major. */
+int igpu_schwarz(const igpu_plan* plan, double* q);
+/* Plan cutoff for IGPU_PRECISION_MIXED (default 1e-4). */
+int igpu_set_mixed_cutoff(igpu_plan* plan, double cutoff);
+
+/* Basis::eri / eri_with (integrals.rs:664-754): dense nao^4 tensor into a
+ * host buffer of nao^4 doubles (assigned). */
+int igpu_eri_dense(igpu_plan* plan, double* out);
+/* EriBuilder::partition + fill (eri_builder.rs:337-417) for the canonical
+ * bra pairs in `bra_subset` (NULL = all): every (ij|kl) over all canonical
+ * ket pairs scattered into the 4 bra/ket-internal slots of the host nao^4
+ * buffer (assigned; other elements untouched). */
+int igpu_eri_builder_fill(igpu_plan* plan, const uint32_t* bra_subset, size_t nsub, double* out);
+
+/* DirectContractor::density_shell_bounds (direct.rs:103-125): per density the
+ * max |D| of every ordered shell block, ndens x nsh x nsh. */
+int igpu_density_shell_bounds(const igpu_plan* plan, const double* dens, int ndens, double* bounds);
+
+/* DirectContractor::accumulate_bra_pair (direct.rs:131-218) over the
+ * canonical bra pairs in bra_subset (NULL = all) in one launch sequence:
+ * J[d] += sum (ab|cd) D[d]_cd, K[d] += sum (ab|cd) D[d]_bd over the
+ * Schwarz/density-screened canonical quartets.  Host buffers; K may be NULL
+ * when want_k == 0. */
+int igpu_jk(igpu_plan* plan, const double* dens, int ndens, const uint32_t* bra_subset, size_t nsub,
+            double threshold, int want_k, int precision, double* J, double* K);
+/* Same with device-resident D, J, K on a caller stream (cudaStream_t). */
+int igpu_jk_device(igpu_plan* plan, const double* d_dens, int ndens, const uint32_t* bra_subset,
+                   size_t nsub, double threshold, int want_k, int precision, double* d_J,
+                   double* d_K, void* stream);
+
+/* DirectGradContractor::density + accumulate_bra_pair / contract
+ * (direct_grad.rs:272-392): out[natom][3] += dE/dR.  Host buffers. */
+int igpu_grad(igpu_plan* plan, const igpu_term* coulomb, int ncoul, const igpu_term* exchange,
+              int nexch, const uint32_t* bra_subset, size_t nsub, double threshold, int precision,
+              double* out);
+/* Same with device-resident term matrices and output on a caller stream. */
+int igpu_grad_device(igpu_plan* plan, const igpu_term* d_coulomb, int ncoul,
+                     const igpu_term* d_exchange, int nexch, const uint32_t* bra_subset,
+                     size_t nsub, double threshold, int precision, double* d_out, void* stream);
+
+/* Counters of the last J/K or gradient call on the plan. */
+int igpu_last_stats(const igpu_plan* plan, igpu_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* INTEGRAL_GPU_H */

@@ -1,0 +1,159 @@
+// Internal data layout shared by the host plan (plan.cpp) and the device
+// kernels (kernels.cu).  Everything here is plain data in device memory.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+namespace igpu {
+
+constexpr int MAX_L = 6;             // reference engine cap (src/engine/os.rs:34)
+constexpr int MAX_GRAD_L = MAX_L - 1;
+constexpr int GPU_MAX_L = 4;         // highest shell l with compiled quartet kernels
+constexpr int MAX_ROOTS = 13;
+constexpr int RYS_NC = 17;           // degree-16 Chebyshev series per root/weight
+constexpr int MAX_DENS = 64;
+constexpr int ADDR_TAB_DEG_HOST = 20;  // degrees of the device triple table
+
+// One shell on the device.
+struct DevShell {
+  double cx, cy, cz;
+  int l;
+  int nprim;
+  int off;       // first function (AO) index
+  int nfunc;     // n_cart or 2l+1
+  int atom;      // index into Basis::atoms()
+  int spherical;
+  int prim_off;  // first primitive in the exponent/coefficient arrays
+  int pad;
+};
+
+// One primitive pair of a shell pair in evaluation orientation (first shell
+// A, second shell B, l_A >= l_B), surviving the 1e-32 pair screen of the
+// reference (src/engine/os_eri.rs:211-244).
+struct PrimPairD {
+  double zeta;       // alpha + beta
+  double alpha;      // exponent on A (gradient raise on A)
+  double beta;       // exponent on B
+  double px, py, pz; // Gaussian product centre
+  double pax, pay, paz;  // P - A
+  double e;          // kappa * c_A * c_B (effective coefficients)
+};
+
+// One canonical shell pair (i >= j in the reference's sense) with its
+// evaluation orientation.
+struct PairD {
+  int a, b;       // evaluation orientation shells (l_a >= l_b)
+  int i, j;       // canonical shells (i >= j)
+  int prim_off;   // into PrimPairD array
+  int nprim;      // surviving primitive pairs
+  int tri;        // i*(i+1)/2 + j
+  int cls;        // pair class index (l_a*(l_a+1)/2 + l_b)
+  double abx, aby, abz;  // A - B
+  double q;       // Schwarz bound Q[i][j]
+};
+
+// Rys table metadata for n roots: finite branch T < t_hi uses n_sub equal
+// subintervals of width `width`; coefficients at `off` laid out as
+// [(sub*n + i)*2 + {0 root, 1 weight}][RYS_NC].
+struct RysMeta {
+  int n_sub;
+  int off;
+  double width;
+  double t_hi;
+};
+
+// Task list of one class-pair launch: for each listed bra (position in the
+// bra class' Q-sorted pair list) kets 0..nket-1 of the ket class' sorted
+// list.  prefix[b] = sum of nket over earlier bras (64-bit).
+struct TaskList {
+  const int* bra_pair;          // pair index per task bra
+  const int* ket_pairs;         // Q-sorted pair indices of the ket class
+  const unsigned long long* prefix;  // nbra + 1 entries
+  const int* ket_start;         // first ket position per bra (NULL = 0)
+  int nbra;
+  unsigned long long total;
+};
+
+// Constant tables every device module needs (uploaded per module).
+struct ConstData {
+  const int* addr_lxyz;
+  int n_addr;
+  const RysMeta* meta;   // MAX_ROOTS + 1 entries
+  const double* lag_x;   // MAX_ROOTS x MAX_ROOTS
+  const double* lag_w;
+  const float* lag_xf;
+  const float* lag_wf;
+  const double* tab;     // device Chebyshev tables
+  const float* tab_f;
+};
+
+// Output modes of the quartet kernels.
+enum Mode : int {
+  MODE_JK = 0,
+  MODE_DENSE = 1,
+  MODE_SCHWARZ = 2,
+  MODE_BUILDER = 3,
+  MODE_GRAD = 4,
+};
+
+struct JKDev {
+  const double* D;       // ndens x nao x nao
+  const double* bounds;  // ndens x nsh x nsh  (density_shell_bounds)
+  double* J;
+  double* K;
+  int ndens;
+  int want_k;
+  int symmetric;         // every density symmetric (bitwise)
+  double threshold;
+};
+
+struct GradDev {
+  // term matrices: nterm x nao x nao for left and right
+  const double* cl;
+  const double* cr;
+  const double* cf;      // factors
+  const double* xl;
+  const double* xr;
+  const double* xf;
+  const double* cl_max;  // per term symmetrised shell-block maxima nsh x nsh
+  const double* cr_max;
+  const double* xl_max;
+  const double* xr_max;
+  int ncoul, nexch;
+  double threshold;
+  double* out;           // natom x 3
+};
+
+struct Counters {
+  unsigned long long quartets;
+  unsigned long long hash;
+  unsigned long long fp32_quartets;
+  unsigned long long prim_quartets;
+  unsigned long long skipped;
+  unsigned long long pad[3];
+};
+
+// Everything a quartet kernel needs.
+struct KernelArgs {
+  const DevShell* shells;
+  const PairD* pairs;
+  const PrimPairD* prims;
+  const double* c2s;     // c2s matrices (ratio folded), c2s_off[l] into it
+  int c2s_off[GPU_MAX_L + 3];
+  int nsh;
+  int nao;
+  TaskList task;
+  int mode;
+  int fp32;              // this launch evaluates in FP32
+  double* scratch;       // per-team slots for the post phase
+  size_t slot_doubles;
+  JKDev jk;
+  GradDev grad;
+  double* dense;         // nao^4 (MODE_DENSE / MODE_BUILDER)
+  double* schwarz_out;   // per pair Q (MODE_SCHWARZ)
+  Counters* counters;
+  int builder_swap;      // builder mode: requested bra is the evaluation ket
+  const unsigned* bra_bitmap;  // optional: reference bra pairs to keep (bit per pair)
+};
+
+}  // namespace igpu

@@ -1,0 +1,155 @@
+// Registry of the per-class quartet kernels (compiled in class_tu.cu, one
+// module per bra pair class) and the small utility kernels (density
+// shell-block bounds, symmetry check).  The host plan (plan.cpp) calls only
+// the functions declared in launch.hpp.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "launch.hpp"
+
+namespace igpu {
+
+constexpr int NPC = (KERNEL_MAX_L + 1) * (KERNEL_MAX_L + 2) / 2;
+
+#define IGPU_DECL(n)                                     \
+  void register_classes_##n(KernelEntry* tab, int npc); \
+  cudaError_t upload_constants_##n(const ConstData& c);
+IGPU_DECL(0)
+IGPU_DECL(1)
+IGPU_DECL(2)
+IGPU_DECL(3)
+IGPU_DECL(4)
+IGPU_DECL(5)
+#if KERNEL_MAX_L >= 3
+IGPU_DECL(6)
+IGPU_DECL(7)
+IGPU_DECL(8)
+IGPU_DECL(9)
+#endif
+#if KERNEL_MAX_L >= 4
+IGPU_DECL(10)
+IGPU_DECL(11)
+IGPU_DECL(12)
+IGPU_DECL(13)
+IGPU_DECL(14)
+#endif
+
+using RegFn = void (*)(KernelEntry*, int);
+using UpFn = cudaError_t (*)(const ConstData&);
+static const RegFn k_reg[NPC] = {
+    register_classes_0, register_classes_1, register_classes_2, register_classes_3, register_classes_4,
+    register_classes_5,
+#if KERNEL_MAX_L >= 3
+    register_classes_6, register_classes_7, register_classes_8, register_classes_9,
+#endif
+#if KERNEL_MAX_L >= 4
+    register_classes_10, register_classes_11, register_classes_12, register_classes_13, register_classes_14,
+#endif
+};
+static const UpFn k_up[NPC] = {
+    upload_constants_0, upload_constants_1, upload_constants_2, upload_constants_3, upload_constants_4,
+    upload_constants_5,
+#if KERNEL_MAX_L >= 3
+    upload_constants_6, upload_constants_7, upload_constants_8, upload_constants_9,
+#endif
+#if KERNEL_MAX_L >= 4
+    upload_constants_10, upload_constants_11, upload_constants_12, upload_constants_13, upload_constants_14,
+#endif
+};
+
+static KernelEntry g_table[NPC * NPC];
+static std::once_flag g_once;
+
+int kernel_npc() { return NPC; }
+
+const KernelEntry* kernel_entry(int pcb, int pck) {
+  std::call_once(g_once, [] {
+    for (int b = 0; b < NPC; ++b) k_reg[b](g_table, NPC);
+    for (auto& e : g_table) {
+      if (!e.valid) continue;
+      cudaFuncSetAttribute(reinterpret_cast<const void*>(e.k64), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           e.smem64);
+      cudaFuncSetAttribute(reinterpret_cast<const void*>(e.k32), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           e.smem32);
+    }
+  });
+  if (pcb < 0 || pck < 0 || pcb >= NPC || pck >= NPC || pcb < pck) return nullptr;
+  const KernelEntry* e = &g_table[pcb * NPC + pck];
+  return e->valid ? e : nullptr;
+}
+
+cudaError_t upload_all_constants(const ConstData& c) {
+  for (int b = 0; b < NPC; ++b) {
+    cudaError_t e = k_up[b](c);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+int blocks_per_sm(const KernelEntry* e, bool fp32) {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, reinterpret_cast<const void*>(fp32 ? e->k32 : e->k64), 128,
+                                                fp32 ? e->smem32 : e->smem64);
+  return n < 1 ? 1 : n;
+}
+
+cudaError_t launch_quartets(const KernelEntry* e, bool fp32, int grid, const KernelArgs& args,
+                            cudaStream_t stream) {
+  auto k = fp32 ? e->k32 : e->k64;
+  int smem = fp32 ? e->smem32 : e->smem64;
+  k<<<grid, 128, smem, stream>>>(args);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ utilities
+
+// max |M| over every ordered shell block (src/direct.rs:103-125); one thread
+// per (matrix, i, j).  With `symmetrise`, block (i,j) takes the max of (i,j)
+// and (j,i) (src/direct_grad.rs:292-312).
+__global__ void shell_block_max_kernel(const double* __restrict__ D, int nmat, const DevShell* __restrict__ sh,
+                                       int nsh, int nao, int symmetrise, double* __restrict__ out) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t per = (size_t)nsh * nsh;
+  if (t >= per * nmat) return;
+  const int d = (int)(t / per);
+  const int r = (int)(t % per);
+  const int i = r / nsh, j = r % nsh;
+  const double* M = D + (size_t)d * nao * nao;
+  const DevShell si = sh[i], sj = sh[j];
+  double mx = 0.0;
+  for (int a = 0; a < si.nfunc; ++a)
+    for (int b = 0; b < sj.nfunc; ++b) mx = fmax(mx, fabs(M[(size_t)(si.off + a) * nao + sj.off + b]));
+  if (symmetrise)
+    for (int a = 0; a < sj.nfunc; ++a)
+      for (int b = 0; b < si.nfunc; ++b) mx = fmax(mx, fabs(M[(size_t)(sj.off + a) * nao + si.off + b]));
+  out[t] = mx;
+}
+
+cudaError_t launch_shell_block_max(const double* D, int nmat, const DevShell* sh, int nsh, int nao,
+                                   int symmetrise, double* out, cudaStream_t s) {
+  const size_t n = (size_t)nsh * nsh * nmat;
+  if (n == 0) return cudaSuccess;
+  shell_block_max_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(D, nmat, sh, nsh, nao, symmetrise, out);
+  return cudaGetLastError();
+}
+
+// flag[0] += 1 for every element with M[r][c] != M[c][r] (bitwise compare).
+__global__ void asym_count_kernel(const double* __restrict__ D, int nmat, int nao, unsigned long long* flag) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t n2 = (size_t)nao * nao;
+  if (t >= n2 * nmat) return;
+  const size_t d = t / n2, r = (t % n2) / nao, c = t % nao;
+  if (c <= r) return;
+  const double* M = D + d * n2;
+  if (__double_as_longlong(M[r * nao + c]) != __double_as_longlong(M[c * nao + r])) atomicAdd(flag, 1ull);
+}
+
+cudaError_t launch_asym_count(const double* D, int nmat, int nao, unsigned long long* flag, cudaStream_t s) {
+  const size_t n = (size_t)nao * nao * nmat;
+  if (n == 0) return cudaSuccess;
+  asym_count_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(D, nmat, nao, flag);
+  return cudaGetLastError();
+}
+
+}  // namespace igpu

@@ -1,0 +1,797 @@
+// Host plan and C ABI (include/integral_gpu.h).
+//
+// The plan mirrors the precompute of the reference's DirectContractor /
+// DirectGradContractor / EriBuilder constructors (src/direct.rs:59-87,
+// src/direct_grad.rs:180-247, src/eri_builder.rs:238-270): shell metadata,
+// AO offsets, atoms, effective coefficients, c2s matrices, canonical shell
+// pairs with their screened primitive-pair data, and the Schwarz bounds —
+// the latter evaluated on the device at creation.  Canonical pairs are
+// bucketed by angular class and sorted by Q so that, for a threshold tau,
+// the kets accepted by Q_bra*Q_ket >= tau form a prefix of every bra's ket
+// list; the per-class task lists are cached per threshold.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/integral_gpu.h"
+#include "grad.hpp"
+#include "host_math.hpp"
+#include "launch.hpp"
+
+using namespace igpu;
+
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* where) {
+  g_err = std::string(where) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? IGPU_ERR_OUT_OF_MEMORY : IGPU_ERR_CUDA;
+}
+#define CK(expr)                                             \
+  do {                                                       \
+    cudaError_t _e = (expr);                                 \
+    if (_e != cudaSuccess) return cuda_fail(_e, #expr);      \
+  } while (0)
+
+int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t ensure(size_t count) {
+    if (count <= n && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+    if (e == cudaSuccess) n = std::max<size_t>(count, 1);
+    return e;
+  }
+  cudaError_t upload(const std::vector<T>& v, cudaStream_t s) {
+    cudaError_t e = ensure(v.size());
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+  }
+};
+
+// One class-pair launch of the quartet kernels.
+struct Launch {
+  int pcb = 0, pck = 0;
+  bool fp32 = false;
+  int builder_swap = 0;
+  int nbra = 0;
+  unsigned long long total = 0;
+  DevBuf<int> bra_pair, ket_start, own_kets;
+  DevBuf<unsigned long long> prefix;
+  const int* ket_list = nullptr;  // device Q-sorted pair list of the ket class
+};
+
+struct TaskSet {
+  std::vector<std::unique_ptr<Launch>> launches;
+};
+
+std::mutex g_const_mutex;
+std::vector<int> g_const_ready;  // per device
+}  // namespace
+
+struct igpu_plan {
+  int device = 0;
+  int engine = 0;
+  int nsh = 0, nao = 0, natom = 0, npairs = 0;
+  bool spherical_any = false;
+  std::vector<DevShell> shells;
+  std::vector<std::array<double, 3>> atoms;
+  std::vector<PairD> pairs;            // canonical order p = tri(i, j)
+  std::vector<PrimPairD> prims;
+  std::vector<double> c2s;
+  int c2s_off[GPU_MAX_L + 3] = {0};
+  std::vector<std::vector<int>> class_pairs;  // per pair class, Q-descending
+  std::vector<double> schwarz;               // nsh x nsh
+  // device
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  DevBuf<DevShell> d_shells;
+  DevBuf<PairD> d_pairs;
+  DevBuf<PrimPairD> d_prims;
+  DevBuf<double> d_c2s;
+  DevBuf<int> d_class_lists;
+  std::vector<int> class_list_off;
+  DevBuf<double> d_scratch;
+  DevBuf<Counters> d_counters;
+  DevBuf<double> d_schwarz_pair;
+  // per-call device buffers
+  DevBuf<double> d_D, d_J, d_K, d_bounds, d_dense;
+  DevBuf<unsigned long long> d_flag;
+  DevBuf<unsigned> d_bitmap;
+  std::map<std::pair<double, double>, std::unique_ptr<TaskSet>> jk_tasks;  // (threshold, fp64 cutoff)
+  std::unique_ptr<TaskSet> dense_tasks;
+  double mixed_cutoff = 1e-4;
+  igpu_stats last{};
+  GradState grad;
+};
+
+namespace {
+
+// Upload the angular tables and the Rys tables to this device once.
+int ensure_constants(int dev) {
+  std::lock_guard<std::mutex> lk(g_const_mutex);
+  if ((int)g_const_ready.size() <= dev) g_const_ready.resize(dev + 1, 0);
+  if (g_const_ready[dev]) return IGPU_OK;
+  const RysTables& T = rys_tables();
+  std::vector<int> lxyz;
+  for (int d = 0; d <= ADDR_TAB_DEG_HOST; ++d)
+    for (auto& c : cart_comps(d)) lxyz.push_back(c[0] | (c[1] << 8) | (c[2] << 16));
+  double* d_tab = nullptr;
+  float* d_tab_f = nullptr;
+  CK(cudaMalloc(&d_tab, T.coef.size() * sizeof(double)));
+  CK(cudaMalloc(&d_tab_f, T.coef.size() * sizeof(float)));
+  std::vector<float> tf(T.coef.begin(), T.coef.end());
+  CK(cudaMemcpy(d_tab, T.coef.data(), T.coef.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_tab_f, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice));
+  float lxf[MAX_ROOTS * MAX_ROOTS], lwf[MAX_ROOTS * MAX_ROOTS];
+  for (int i = 0; i < MAX_ROOTS * MAX_ROOTS; ++i) {
+    lxf[i] = (float)T.lag_x[i];
+    lwf[i] = (float)T.lag_w[i];
+  }
+  ConstData c;
+  c.addr_lxyz = lxyz.data();
+  c.n_addr = (int)lxyz.size();
+  c.meta = T.meta.data();
+  c.lag_x = T.lag_x;
+  c.lag_w = T.lag_w;
+  c.lag_xf = lxf;
+  c.lag_wf = lwf;
+  c.tab = d_tab;
+  c.tab_f = d_tab_f;
+  CK(upload_all_constants(c));
+  g_const_ready[dev] = 1;
+  return IGPU_OK;
+}
+
+size_t grid_for(const KernelEntry* e, bool fp32, unsigned long long total) {
+  static int nsm = 0;
+  if (!nsm) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (nsm <= 0) nsm = 1;
+  }
+  const int teams_per_block = 128 / e->team;
+  const unsigned long long need = (total + teams_per_block - 1) / teams_per_block;
+  const unsigned long long cap = (unsigned long long)blocks_per_sm(e, fp32) * nsm;
+  return (size_t)std::max<unsigned long long>(1, std::min(need, cap));
+}
+
+KernelArgs base_args(igpu_plan* P) {
+  KernelArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.shells = P->d_shells.p;
+  A.pairs = P->d_pairs.p;
+  A.prims = P->d_prims.p;
+  A.c2s = P->d_c2s.p;
+  for (int l = 0; l < GPU_MAX_L + 3; ++l) A.c2s_off[l] = P->c2s_off[l];
+  A.nsh = P->nsh;
+  A.nao = P->nao;
+  A.counters = P->d_counters.p;
+  return A;
+}
+
+// Run every launch of a task set in `mode`; quartet kernels only.
+int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t& launches) {
+  for (auto& L : ts.launches) {
+    if (L->total == 0) continue;
+    const KernelEntry* e = kernel_entry(L->pcb, L->pck);
+    if (!e) return fail(IGPU_ERR_UNSUPPORTED, "angular class not compiled for the GPU");
+    const size_t grid = grid_for(e, L->fp32, L->total);
+    const size_t teams = grid * (128 / e->team);
+    CK(P->d_scratch.ensure(teams * e->slot));
+    A.scratch = P->d_scratch.p;
+    A.slot_doubles = e->slot;
+    A.task.bra_pair = L->bra_pair.p;
+    A.task.ket_pairs = L->ket_list;
+    A.task.prefix = L->prefix.p;
+    A.task.ket_start = L->ket_start.n ? L->ket_start.p : nullptr;
+    A.task.nbra = L->nbra;
+    A.task.total = L->total;
+    A.fp32 = L->fp32 ? 1 : 0;
+    A.builder_swap = L->builder_swap;
+    CK(launch_quartets(e, L->fp32, (int)grid, A, s));
+    ++launches;
+  }
+  return IGPU_OK;
+}
+
+// Build one Launch from host vectors.
+std::unique_ptr<Launch> make_launch(igpu_plan* P, int pcb, int pck, bool fp32, const std::vector<int>& bras,
+                                    const std::vector<int>& nket, const std::vector<int>& kstart,
+                                    const int* ket_list_dev, int swap, cudaStream_t s, int& rc) {
+  auto L = std::make_unique<Launch>();
+  L->pcb = pcb;
+  L->pck = pck;
+  L->fp32 = fp32;
+  L->builder_swap = swap;
+  std::vector<int> b;
+  std::vector<int> ks;
+  std::vector<unsigned long long> pre(1, 0);
+  for (size_t x = 0; x < bras.size(); ++x) {
+    if (nket[x] <= 0) continue;
+    b.push_back(bras[x]);
+    ks.push_back(kstart.empty() ? 0 : kstart[x]);
+    pre.push_back(pre.back() + (unsigned long long)nket[x]);
+  }
+  L->nbra = (int)b.size();
+  L->total = pre.back();
+  L->ket_list = ket_list_dev;
+  rc = IGPU_OK;
+  cudaError_t e;
+  if ((e = L->bra_pair.upload(b, s)) || (e = L->prefix.upload(pre, s))) {
+    rc = cuda_fail(e, "task upload");
+    return nullptr;
+  }
+  bool any_start = std::any_of(ks.begin(), ks.end(), [](int v) { return v != 0; });
+  if (any_start && (e = L->ket_start.upload(ks, s))) {
+    rc = cuda_fail(e, "task upload");
+    return nullptr;
+  }
+  return L;
+}
+
+// Screened J/K task lists for threshold tau: for every class pair (CA >= CB)
+// and bra of CA, the kets of CB with Q_bra*Q_ket >= tau (a prefix of the
+// Q-sorted list; the upper triangle when CA == CB).  With fp64_cut > 0 the
+// prefix is split: kets with Q_bra*Q_ket >= fp64_cut run in FP64, the rest in
+// FP32.
+int build_jk_tasks(igpu_plan* P, double tau, double fp64_cut, TaskSet& ts) {
+  const int npc = (int)P->class_pairs.size();
+  for (int ca = 0; ca < npc; ++ca)
+    for (int cb = 0; cb <= ca; ++cb) {
+      const auto& B = P->class_pairs[ca];
+      const auto& K = P->class_pairs[cb];
+      if (B.empty() || K.empty()) continue;
+      std::vector<double> qk(K.size());
+      for (size_t x = 0; x < K.size(); ++x) qk[x] = P->pairs[K[x]].q;
+      std::vector<int> bras(B.size()), n64(B.size()), n32(B.size()), st32(B.size());
+      for (size_t bp = 0; bp < B.size(); ++bp) {
+        const double qb = P->pairs[B[bp]].q;
+        // first ket with qb*qk < tau
+        size_t lo = 0, hi = K.size();
+        while (lo < hi) {
+          size_t mid = (lo + hi) / 2;
+          if (qb * qk[mid] >= tau)
+            lo = mid + 1;
+          else
+            hi = mid;
+        }
+        size_t nk = lo;
+        if (ca == cb) nk = std::min(nk, bp + 1);
+        size_t split = nk;
+        if (fp64_cut > 0.0) {
+          size_t l2 = 0, h2 = nk;
+          while (l2 < h2) {
+            size_t mid = (l2 + h2) / 2;
+            if (qb * qk[mid] >= fp64_cut)
+              l2 = mid + 1;
+            else
+              h2 = mid;
+          }
+          split = l2;
+        }
+        bras[bp] = B[bp];
+        n64[bp] = (int)split;
+        n32[bp] = (int)(nk - split);
+        st32[bp] = (int)split;
+      }
+      const int* klist = P->d_class_lists.p + P->class_list_off[cb];
+      int rc;
+      auto L64 = make_launch(P, ca, cb, false, bras, n64, {}, klist, 0, P->stream, rc);
+      if (!L64) return rc;
+      ts.launches.push_back(std::move(L64));
+      if (fp64_cut > 0.0) {
+        auto L32 = make_launch(P, ca, cb, true, bras, n32, st32, klist, 0, P->stream, rc);
+        if (!L32) return rc;
+        ts.launches.push_back(std::move(L32));
+      }
+    }
+  return IGPU_OK;
+}
+
+int check_bra_subset(igpu_plan* P, const uint32_t* sub, size_t nsub, std::vector<unsigned>& bitmap) {
+  bitmap.assign(((size_t)P->npairs + 31) / 32, 0u);
+  for (size_t x = 0; x < nsub; ++x) {
+    if (sub[x] >= (uint32_t)P->npairs) return fail(IGPU_ERR_NONCANONICAL_BRA, "bra pair index out of range");
+    bitmap[sub[x] / 32] |= 1u << (sub[x] % 32);
+  }
+  return IGPU_OK;
+}
+
+int run_schwarz(igpu_plan* P) {
+  // one (P|P) quartet per canonical pair, no screening
+  TaskSet ts;
+  const int npc = (int)P->class_pairs.size();
+  for (int c = 0; c < npc; ++c) {
+    const auto& B = P->class_pairs[c];
+    if (B.empty()) continue;
+    std::vector<int> nk(B.size(), 1), ks(B.size());
+    std::iota(ks.begin(), ks.end(), 0);
+    int rc;
+    auto L = make_launch(P, c, c, false, B, nk, ks, P->d_class_lists.p + P->class_list_off[c], 0, P->stream, rc);
+    if (!L) return rc;
+    ts.launches.push_back(std::move(L));
+  }
+  CK(P->d_schwarz_pair.ensure(P->npairs));
+  KernelArgs A = base_args(P);
+  A.mode = MODE_SCHWARZ;
+  A.schwarz_out = P->d_schwarz_pair.p;
+  A.counters = nullptr;
+  uint32_t launches = 0;
+  int rc = run_tasks(P, ts, A, P->stream, launches);
+  if (rc) return rc;
+  std::vector<double> q(P->npairs);
+  CK(cudaMemcpyAsync(q.data(), P->d_schwarz_pair.p, q.size() * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
+  CK(cudaStreamSynchronize(P->stream));
+  P->schwarz.assign((size_t)P->nsh * P->nsh, 0.0);
+  for (int p = 0; p < P->npairs; ++p) {
+    P->pairs[p].q = q[p];
+    const int i = P->pairs[p].i, j = P->pairs[p].j;
+    P->schwarz[(size_t)i * P->nsh + j] = q[p];
+    P->schwarz[(size_t)j * P->nsh + i] = q[p];
+  }
+  return IGPU_OK;
+}
+
+}  // namespace
+
+// ===================================================================== C ABI
+
+extern "C" {
+
+uint32_t igpu_abi_version(void) { return IGPU_ABI_VERSION; }
+
+const char* igpu_last_error_string(void) { return g_err.c_str(); }
+
+int igpu_plan_create(const igpu_shell* sh, size_t nsh, int engine, igpu_plan** out) {
+  if (!out) return fail(IGPU_ERR_INVALID_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  if (nsh > 0 && !sh) return fail(IGPU_ERR_INVALID_ARGUMENT, "shells is NULL");
+  if (engine < 0 || engine > 2) return fail(IGPU_ERR_INVALID_ARGUMENT, "unknown engine");
+  if (nsh > 65535) return fail(IGPU_ERR_INVALID_ARGUMENT, "at most 65535 shells");
+  // validation order of Shell::with_kind (src/shell.rs:92-118)
+  for (size_t s = 0; s < nsh; ++s) {
+    if (sh[s].nprim <= 0) return fail(IGPU_ERR_EMPTY_CONTRACTION, "shell has no primitives");
+    if (!sh[s].exps || !sh[s].coefs) return fail(IGPU_ERR_INVALID_ARGUMENT, "shell exponents/coefficients NULL");
+    if (sh[s].l < 0) return fail(IGPU_ERR_INVALID_ARGUMENT, "negative angular momentum");
+    if (sh[s].l > MAX_L) return fail(IGPU_ERR_ANGULAR_MOMENTUM, "angular momentum exceeds supported maximum 6");
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(IGPU_ERR_NO_DEVICE, "no CUDA device");
+  }
+  auto P = std::make_unique<igpu_plan>();
+  CK(cudaGetDevice(&P->device));
+  P->engine = engine;
+  P->nsh = (int)nsh;
+  int rc = ensure_constants(P->device);
+  if (rc) return rc;
+  // shells, offsets, atoms (shell.rs:193-262)
+  std::vector<double> eff;
+  std::vector<double> expv;
+  int acc = 0;
+  for (size_t s = 0; s < nsh; ++s) {
+    DevShell d{};
+    d.cx = sh[s].center[0];
+    d.cy = sh[s].center[1];
+    d.cz = sh[s].center[2];
+    d.l = sh[s].l;
+    d.nprim = sh[s].nprim;
+    d.spherical = sh[s].spherical ? 1 : 0;
+    d.nfunc = d.spherical ? 2 * d.l + 1 : (d.l + 1) * (d.l + 2) / 2;
+    d.off = acc;
+    acc += d.nfunc;
+    d.prim_off = (int)expv.size();
+    for (int p = 0; p < d.nprim; ++p) {
+      expv.push_back(sh[s].exps[p]);
+      eff.push_back(effective_coeff(sh[s].exps[p], sh[s].coefs[p], d.l));
+    }
+    int atom = -1;
+    for (size_t a = 0; a < P->atoms.size(); ++a)
+      if (P->atoms[a][0] == d.cx && P->atoms[a][1] == d.cy && P->atoms[a][2] == d.cz) atom = (int)a;
+    if (atom < 0) {
+      atom = (int)P->atoms.size();
+      P->atoms.push_back({d.cx, d.cy, d.cz});
+    }
+    d.atom = atom;
+    if (d.spherical) P->spherical_any = true;
+    P->shells.push_back(d);
+  }
+  P->nao = acc;
+  P->natom = (int)P->atoms.size();
+  int lmax = 0;
+  for (auto& d : P->shells) lmax = std::max(lmax, d.l);
+  if (lmax > KERNEL_MAX_L)
+    return fail(IGPU_ERR_UNSUPPORTED, "shell angular momentum above the compiled GPU classes (l <= " +
+                                          std::to_string(KERNEL_MAX_L) + ")");
+  // c2s matrices (l <= GPU_MAX_L + 1)
+  for (int l = 0; l <= GPU_MAX_L + 1; ++l) {
+    P->c2s_off[l] = (int)P->c2s.size();
+    auto m = c2s_effective(l);
+    P->c2s.insert(P->c2s.end(), m.begin(), m.end());
+  }
+  P->c2s_off[GPU_MAX_L + 2] = (int)P->c2s.size();
+  // canonical pairs (integrals.rs:1252-1260) and primitive-pair data in
+  // evaluation orientation (l_a >= l_b), screened as os_eri.rs:211-244
+  const int npc = pair_class(lmax, lmax) + 1;
+  P->class_pairs.assign(npc, {});
+  for (int i = 0; i < (int)nsh; ++i)
+    for (int j = 0; j <= i; ++j) {
+      const DevShell& si = P->shells[i];
+      const DevShell& sj = P->shells[j];
+      const bool keep = si.l >= sj.l;
+      const DevShell& A = keep ? si : sj;
+      const DevShell& B = keep ? sj : si;
+      PairD pr{};
+      pr.a = keep ? i : j;
+      pr.b = keep ? j : i;
+      pr.i = i;
+      pr.j = j;
+      pr.tri = i * (i + 1) / 2 + j;
+      pr.cls = pair_class(A.l, B.l);
+      pr.abx = A.cx - B.cx;
+      pr.aby = A.cy - B.cy;
+      pr.abz = A.cz - B.cz;
+      pr.prim_off = (int)P->prims.size();
+      const double d2 = pr.abx * pr.abx + pr.aby * pr.aby + pr.abz * pr.abz;
+      for (int pa = 0; pa < A.nprim; ++pa)
+        for (int pb = 0; pb < B.nprim; ++pb) {
+          const double ea = expv[A.prim_off + pa], eb = expv[B.prim_off + pb];
+          const double ca = eff[A.prim_off + pa], cb = eff[B.prim_off + pb];
+          const double z = ea + eb;
+          const double kappa = std::exp(-(ea * eb / z) * d2);
+          if (kappa * std::fabs(ca * cb) < 1e-32) continue;
+          PrimPairD q{};
+          q.zeta = z;
+          q.alpha = ea;
+          q.beta = eb;
+          q.px = (ea * A.cx + eb * B.cx) / z;
+          q.py = (ea * A.cy + eb * B.cy) / z;
+          q.pz = (ea * A.cz + eb * B.cz) / z;
+          q.pax = q.px - A.cx;
+          q.pay = q.py - A.cy;
+          q.paz = q.pz - A.cz;
+          q.e = kappa * ca * cb;
+          P->prims.push_back(q);
+        }
+      pr.nprim = (int)P->prims.size() - pr.prim_off;
+      P->pairs.push_back(pr);
+      P->class_pairs[pr.cls].push_back((int)P->pairs.size() - 1);
+    }
+  P->npairs = (int)P->pairs.size();
+  P->grad.expv = expv;
+  P->grad.eff = eff;
+  CK(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&P->ev0));
+  CK(cudaEventCreate(&P->ev1));
+  CK(P->d_shells.upload(P->shells, P->stream));
+  CK(P->d_pairs.upload(P->pairs, P->stream));
+  CK(P->d_prims.upload(P->prims, P->stream));
+  CK(P->d_c2s.upload(P->c2s, P->stream));
+  CK(P->d_counters.ensure(1));
+  // class lists (device) in pair order for the Schwarz pass
+  {
+    std::vector<int> flat;
+    P->class_list_off.assign(npc, 0);
+    for (int c = 0; c < npc; ++c) {
+      P->class_list_off[c] = (int)flat.size();
+      flat.insert(flat.end(), P->class_pairs[c].begin(), P->class_pairs[c].end());
+    }
+    CK(P->d_class_lists.upload(flat, P->stream));
+  }
+  rc = run_schwarz(P.get());
+  if (rc) return rc;
+  // re-sort every class by Q descending (stable on pair index) for screening
+  {
+    std::vector<int> flat;
+    for (int c = 0; c < npc; ++c) {
+      auto& v = P->class_pairs[c];
+      std::stable_sort(v.begin(), v.end(), [&](int x, int y) { return P->pairs[x].q > P->pairs[y].q; });
+      P->class_list_off[c] = (int)flat.size();
+      flat.insert(flat.end(), v.begin(), v.end());
+    }
+    CK(P->d_pairs.upload(P->pairs, P->stream));
+    CK(P->d_class_lists.upload(flat, P->stream));
+    CK(cudaStreamSynchronize(P->stream));
+  }
+  *out = P.release();
+  return IGPU_OK;
+}
+
+int igpu_plan_destroy(igpu_plan* plan) {
+  if (!plan) return IGPU_OK;
+  cudaStreamSynchronize(plan->stream);
+  if (plan->ev0) cudaEventDestroy(plan->ev0);
+  if (plan->ev1) cudaEventDestroy(plan->ev1);
+  cudaStream_t s = plan->stream;
+  delete plan;
+  if (s) cudaStreamDestroy(s);
+  return IGPU_OK;
+}
+
+int igpu_plan_query(const igpu_plan* P, size_t* nao, size_t* natom, size_t* nbra, size_t* nsh) {
+  if (!P) return fail(IGPU_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (nao) *nao = P->nao;
+  if (natom) *natom = P->natom;
+  if (nbra) *nbra = P->npairs;
+  if (nsh) *nsh = P->nsh;
+  return IGPU_OK;
+}
+
+int igpu_bra_pairs(const igpu_plan* P, uint32_t* out) {
+  if (!P || !out) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  for (int p = 0; p < P->npairs; ++p) {
+    out[2 * p] = P->pairs[p].i;
+    out[2 * p + 1] = P->pairs[p].j;
+  }
+  return IGPU_OK;
+}
+
+int igpu_atoms(const igpu_plan* P, double* xyz) {
+  if (!P || !xyz) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  for (int a = 0; a < P->natom; ++a)
+    for (int c = 0; c < 3; ++c) xyz[3 * a + c] = P->atoms[a][c];
+  return IGPU_OK;
+}
+
+int igpu_schwarz(const igpu_plan* P, double* q) {
+  if (!P || !q) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::memcpy(q, P->schwarz.data(), P->schwarz.size() * sizeof(double));
+  return IGPU_OK;
+}
+
+int igpu_set_mixed_cutoff(igpu_plan* P, double cutoff) {
+  if (!P || !(cutoff >= 0.0)) return fail(IGPU_ERR_INVALID_ARGUMENT, "invalid cutoff");
+  P->mixed_cutoff = cutoff;
+  return IGPU_OK;
+}
+
+int igpu_density_shell_bounds(const igpu_plan* Pc, const double* dens, int ndens, double* bounds) {
+  igpu_plan* P = const_cast<igpu_plan*>(Pc);
+  if (!P || !dens || !bounds) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (ndens < 1 || ndens > MAX_DENS) return fail(IGPU_ERR_DENSITY_COUNT, "1..64 densities");
+  const size_t n2 = (size_t)P->nao * P->nao;
+  CK(P->d_D.ensure(n2 * ndens));
+  CK(P->d_bounds.ensure((size_t)P->nsh * P->nsh * ndens));
+  CK(cudaMemcpyAsync(P->d_D.p, dens, n2 * ndens * sizeof(double), cudaMemcpyHostToDevice, P->stream));
+  CK(launch_shell_block_max(P->d_D.p, ndens, P->d_shells.p, P->nsh, P->nao, 0, P->d_bounds.p, P->stream));
+  CK(cudaMemcpyAsync(bounds, P->d_bounds.p, (size_t)P->nsh * P->nsh * ndens * sizeof(double),
+                     cudaMemcpyDeviceToHost, P->stream));
+  CK(cudaStreamSynchronize(P->stream));
+  return IGPU_OK;
+}
+
+int igpu_jk_device(igpu_plan* P, const double* d_dens, int ndens, const uint32_t* bra_subset, size_t nsub,
+                   double threshold, int want_k, int precision, double* d_J, double* d_K, void* stream) {
+  if (!P || !d_dens || !d_J) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (ndens < 1 || ndens > MAX_DENS) return fail(IGPU_ERR_DENSITY_COUNT, "1..64 densities");
+  if (want_k && !d_K) return fail(IGPU_ERR_INVALID_ARGUMENT, "exchange buffer required");
+  if (precision != IGPU_PRECISION_FP64 && precision != IGPU_PRECISION_MIXED)
+    return fail(IGPU_ERR_INVALID_ARGUMENT, "unknown precision");
+  if (std::isnan(threshold)) return fail(IGPU_ERR_INVALID_ARGUMENT, "threshold is NaN");
+  cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
+  std::vector<unsigned> bitmap;
+  if (bra_subset) {
+    int rc = check_bra_subset(P, bra_subset, nsub, bitmap);
+    if (rc) return rc;
+    CK(P->d_bitmap.ensure(bitmap.size()));
+    CK(cudaMemcpyAsync(P->d_bitmap.p, bitmap.data(), bitmap.size() * sizeof(unsigned), cudaMemcpyHostToDevice, s));
+  }
+  const size_t nn = (size_t)P->nsh * P->nsh;
+  CK(P->d_bounds.ensure(nn * ndens));
+  CK(P->d_flag.ensure(1));
+  CK(cudaMemsetAsync(P->d_flag.p, 0, sizeof(unsigned long long), s));
+  CK(launch_shell_block_max(d_dens, ndens, P->d_shells.p, P->nsh, P->nao, 0, P->d_bounds.p, s));
+  CK(launch_asym_count(d_dens, ndens, P->nao, P->d_flag.p, s));
+  unsigned long long asym = 0;
+  CK(cudaMemcpyAsync(&asym, P->d_flag.p, sizeof(asym), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemsetAsync(P->d_counters.p, 0, sizeof(Counters), s));
+  // FP64 part: Q_bra*Q_ket*max|D| >= cutoff (the bounds' global max)
+  double fp64_cut = 0.0;
+  if (precision == IGPU_PRECISION_MIXED) {
+    std::vector<double> hb(nn * ndens);
+    CK(cudaMemcpyAsync(hb.data(), P->d_bounds.p, hb.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    double dmax = 0.0;
+    for (double v : hb) dmax = std::max(dmax, v);
+    fp64_cut = dmax > 0.0 ? P->mixed_cutoff / dmax : std::numeric_limits<double>::infinity();
+    if (fp64_cut <= 0.0) fp64_cut = std::numeric_limits<double>::min();
+  } else {
+    CK(cudaStreamSynchronize(s));
+  }
+  auto key = std::make_pair(threshold, fp64_cut);
+  auto it = P->jk_tasks.find(key);
+  if (it == P->jk_tasks.end()) {
+    auto ts = std::make_unique<TaskSet>();
+    int rc = build_jk_tasks(P, threshold, fp64_cut, *ts);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(P->stream));
+    it = P->jk_tasks.emplace(key, std::move(ts)).first;
+  }
+  KernelArgs A = base_args(P);
+  A.mode = MODE_JK;
+  A.jk.D = d_dens;
+  A.jk.bounds = P->d_bounds.p;
+  A.jk.J = d_J;
+  A.jk.K = want_k ? d_K : nullptr;
+  A.jk.ndens = ndens;
+  A.jk.want_k = want_k ? 1 : 0;
+  A.jk.symmetric = asym == 0 ? 1 : 0;
+  A.jk.threshold = threshold;
+  A.bra_bitmap = bra_subset ? P->d_bitmap.p : nullptr;
+  uint32_t launches = 3;
+  CK(cudaEventRecord(P->ev0, s));
+  int rc = run_tasks(P, *it->second, A, s, launches);
+  if (rc) return rc;
+  CK(cudaEventRecord(P->ev1, s));
+  Counters c{};
+  CK(cudaMemcpyAsync(&c, P->d_counters.p, sizeof(c), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, P->ev0, P->ev1);
+  P->last = igpu_stats{};
+  P->last.quartets = c.quartets;
+  P->last.quartet_hash = c.hash;
+  P->last.quartets_fp32 = c.fp32_quartets;
+  P->last.prim_quartets = c.prim_quartets;
+  P->last.kernel_ms = ms;
+  P->last.launches = launches;
+  return IGPU_OK;
+}
+
+int igpu_jk(igpu_plan* P, const double* dens, int ndens, const uint32_t* bra_subset, size_t nsub, double threshold,
+            int want_k, int precision, double* J, double* K) {
+  if (!P || !dens || !J) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (ndens < 1 || ndens > MAX_DENS) return fail(IGPU_ERR_DENSITY_COUNT, "1..64 densities");
+  if (want_k && !K) return fail(IGPU_ERR_INVALID_ARGUMENT, "exchange buffer required");
+  const size_t n2 = (size_t)P->nao * P->nao * ndens;
+  CK(P->d_D.ensure(n2));
+  CK(P->d_J.ensure(n2));
+  if (want_k) CK(P->d_K.ensure(n2));
+  CK(cudaMemcpyAsync(P->d_D.p, dens, n2 * sizeof(double), cudaMemcpyHostToDevice, P->stream));
+  CK(cudaMemsetAsync(P->d_J.p, 0, n2 * sizeof(double), P->stream));
+  if (want_k) CK(cudaMemsetAsync(P->d_K.p, 0, n2 * sizeof(double), P->stream));
+  int rc = igpu_jk_device(P, P->d_D.p, ndens, bra_subset, nsub, threshold, want_k, precision, P->d_J.p,
+                          want_k ? P->d_K.p : nullptr, P->stream);
+  if (rc) return rc;
+  std::vector<double> tj(n2), tk(want_k ? n2 : 0);
+  CK(cudaMemcpyAsync(tj.data(), P->d_J.p, n2 * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
+  if (want_k) CK(cudaMemcpyAsync(tk.data(), P->d_K.p, n2 * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
+  CK(cudaStreamSynchronize(P->stream));
+  for (size_t e = 0; e < n2; ++e) J[e] += tj[e];
+  if (want_k)
+    for (size_t e = 0; e < n2; ++e) K[e] += tk[e];
+  return IGPU_OK;
+}
+
+// Dense tensor (MODE_DENSE, every canonical quartet, no screening) or the
+// EriBuilder fill (MODE_BUILDER, every ket for the requested bras).
+static int dense_like(igpu_plan* P, bool builder, const uint32_t* sub, size_t nsub, double* out) {
+  if (!P || !out) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  const size_t n = (size_t)P->nao;
+  const size_t n4 = n * n * n * n;
+  CK(P->d_dense.ensure(n4));
+  if (builder)
+    CK(cudaMemcpyAsync(P->d_dense.p, out, n4 * sizeof(double), cudaMemcpyHostToDevice, P->stream));
+  else
+    CK(cudaMemsetAsync(P->d_dense.p, 0, n4 * sizeof(double), P->stream));
+  TaskSet local;
+  TaskSet* ts = &local;
+  const int npc = (int)P->class_pairs.size();
+  int rc = IGPU_OK;
+  if (!builder) {
+    if (!P->dense_tasks) {
+      P->dense_tasks = std::make_unique<TaskSet>();
+      rc = build_jk_tasks(P, -std::numeric_limits<double>::infinity(), 0.0, *P->dense_tasks);
+      if (rc) return rc;
+    }
+    ts = P->dense_tasks.get();
+  } else {
+    std::vector<char> want(P->npairs, sub ? 0 : 1);
+    for (size_t x = 0; sub && x < nsub; ++x) {
+      if (sub[x] >= (uint32_t)P->npairs) return fail(IGPU_ERR_NONCANONICAL_BRA, "bra pair index out of range");
+      want[sub[x]] = 1;
+    }
+    for (int ca = 0; ca < npc; ++ca)
+      for (int cb = 0; cb <= ca; ++cb) {
+        const auto& A = P->class_pairs[ca];
+        const auto& B = P->class_pairs[cb];
+        if (A.empty() || B.empty()) continue;
+        // requested bras of class ca, every ket of class cb
+        std::vector<int> bras, nk;
+        for (int p : A)
+          if (want[p]) {
+            bras.push_back(p);
+            nk.push_back((int)B.size());
+          }
+        auto L = make_launch(P, ca, cb, false, bras, nk, {}, P->d_class_lists.p + P->class_list_off[cb], 0,
+                             P->stream, rc);
+        if (!L) return rc;
+        local.launches.push_back(std::move(L));
+        if (ca != cb) {
+          // requested bras of class cb: evaluated as (ket of ca | bra)
+          std::vector<int> reqs;
+          for (int p : B)
+            if (want[p]) reqs.push_back(p);
+          if (reqs.empty()) continue;
+          auto L2 = std::make_unique<Launch>();
+          L2->pcb = ca;
+          L2->pck = cb;
+          L2->builder_swap = 1;
+          std::vector<int> br(A.begin(), A.end());
+          std::vector<unsigned long long> pre(1, 0);
+          for (size_t x = 0; x < br.size(); ++x) pre.push_back(pre.back() + reqs.size());
+          L2->nbra = (int)br.size();
+          L2->total = pre.back();
+          CK(L2->bra_pair.upload(br, P->stream));
+          CK(L2->prefix.upload(pre, P->stream));
+          // ket list = the requested bras (device copy owned by the launch)
+          CK(L2->own_kets.upload(reqs, P->stream));
+          L2->ket_list = L2->own_kets.p;
+          local.launches.push_back(std::move(L2));
+        }
+      }
+  }
+  KernelArgs A = base_args(P);
+  A.mode = builder ? MODE_BUILDER : MODE_DENSE;
+  A.dense = P->d_dense.p;
+  A.counters = nullptr;
+  uint32_t launches = 0;
+  rc = run_tasks(P, *ts, A, P->stream, launches);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(out, P->d_dense.p, n4 * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
+  CK(cudaStreamSynchronize(P->stream));
+  P->last = igpu_stats{};
+  P->last.launches = launches;
+  return IGPU_OK;
+}
+
+int igpu_eri_dense(igpu_plan* P, double* out) { return dense_like(P, false, nullptr, 0, out); }
+
+int igpu_eri_builder_fill(igpu_plan* P, const uint32_t* sub, size_t nsub, double* out) {
+  return dense_like(P, true, sub, nsub, out);
+}
+
+int igpu_last_stats(const igpu_plan* P, igpu_stats* st) {
+  if (!P || !st) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  *st = P->last;
+  return IGPU_OK;
+}
+
+int igpu_grad(igpu_plan* P, const igpu_term* coulomb, int ncoul, const igpu_term* exchange, int nexch,
+              const uint32_t* bra_subset, size_t nsub, double threshold, int precision, double* out) {
+  return grad_host(P, coulomb, ncoul, exchange, nexch, bra_subset, nsub, threshold, precision, out);
+}
+
+int igpu_grad_device(igpu_plan* P, const igpu_term* d_coulomb, int ncoul, const igpu_term* d_exchange, int nexch,
+                     const uint32_t* bra_subset, size_t nsub, double threshold, int precision, double* d_out,
+                     void* stream) {
+  return grad_device(P, d_coulomb, ncoul, d_exchange, nexch, bra_subset, nsub, threshold, precision, d_out, stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,473 @@
+// Task decoding, screening, and the per-quartet post phase (horizontal
+// recurrences on the contracted table, Cartesian -> spherical transform, and
+// the consumers: J/K contraction, dense 8-fold scatter, EriBuilder 4-fold
+// scatter, Schwarz diagonal maximum).  Runs on a team of T lanes over a
+// per-team scratch slot in global memory.
+#pragma once
+#include "device_common.cuh"
+
+namespace igpu {
+
+struct ClassDims {
+  int la, lb, lc, ld;
+};
+
+// Scratch-slot layout of one quartet (in doubles): three level buffers of S
+// doubles (the first holds G on entry), then the Cartesian block and its
+// transform partner.
+struct SlotLayout {
+  size_t S, blk, total;
+};
+__host__ __device__ inline SlotLayout slot_layout(int la, int lb, int lc, int ld) {
+  int ne = la + lb, nf = lc + ld;
+  int nep = nrange(la, ne), nfp = nrange(lc, nf);
+  size_t S = (size_t)nep * nfp;
+  for (int kb = 1; kb <= lb; ++kb) {
+    size_t s = (size_t)ncart(kb) * nrange(la, ne - kb) * nfp;
+    S = s > S ? s : S;
+  }
+  size_t nab = (size_t)ncart(la) * ncart(lb);
+  for (int kd = 1; kd <= ld; ++kd) {
+    size_t s = nab * ncart(kd) * nrange(lc, nf - kd);
+    S = s > S ? s : S;
+  }
+  size_t blk = nab * ncart(lc) * ncart(ld);
+  SlotLayout L;
+  L.S = S;
+  L.blk = blk;
+  L.total = 3 * S + 2 * blk;
+  return L;
+}
+
+__device__ __forceinline__ void decode_task(const TaskList& t, unsigned long long g, int& pbi, int& pki) {
+  int lo = 0, hi = t.nbra;  // prefix[lo] <= g < prefix[hi]
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (t.prefix[mid] <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  int kpos = (int)(g - t.prefix[lo]) + (t.ket_start ? t.ket_start[lo] : 0);
+  pbi = t.bra_pair[lo];
+  pki = t.ket_pairs[kpos];
+}
+
+struct Screen {
+  bool keep;
+  bool swapped;       // reference bra is the evaluation ket pair
+  uint64_t mask;      // densities this quartet contributes to
+  int i, j, k, l;     // reference canonical shells
+};
+
+// Reference screening of one canonical quartet.  The reference bra is the
+// pair with the larger canonical index (its loops run k <= i, l <= l_top,
+// src/direct.rs:169-190); the Schwarz product Q_ij*Q_kl and the density
+// mask max(|D| over the six blocks) are evaluated in that orientation so the
+// accepted list is the reference's, bit for bit.
+__device__ __forceinline__ Screen screen_quartet(const KernelArgs& A, const PairD& pb, const PairD& pk) {
+  Screen s;
+  s.swapped = pk.tri > pb.tri;
+  const PairD& rb = s.swapped ? pk : pb;
+  const PairD& rk = s.swapped ? pb : pk;
+  s.i = rb.i;
+  s.j = rb.j;
+  s.k = rk.i;
+  s.l = rk.j;
+  s.mask = 1;
+  s.keep = true;
+  if (A.bra_bitmap && !((__ldg(A.bra_bitmap + (rb.tri >> 5)) >> (rb.tri & 31)) & 1u)) {
+    s.keep = false;
+    return s;
+  }
+  if (A.mode == MODE_JK) {
+    const double qab = rb.q;
+    if (qab == 0.0) {  // direct.rs:166, unconditional
+      s.keep = false;
+      return s;
+    }
+    const double pair_bound = qab * rk.q;
+    if (pair_bound < A.jk.threshold) {
+      s.keep = false;
+      return s;
+    }
+    const int n = A.nsh;
+    uint64_t mask = 0;
+    for (int d = 0; d < A.jk.ndens; ++d) {
+      const double* bd = A.jk.bounds + (size_t)d * n * n;
+      double db = fmax(fmax(fmax(fmax(fmax(__ldg(bd + (size_t)s.i * n + s.j), __ldg(bd + (size_t)s.k * n + s.l)),
+                                      __ldg(bd + (size_t)s.i * n + s.k)),
+                                 __ldg(bd + (size_t)s.i * n + s.l)),
+                            __ldg(bd + (size_t)s.j * n + s.k)),
+                       __ldg(bd + (size_t)s.j * n + s.l));
+      if (pair_bound * db >= A.jk.threshold) mask |= 1ull << d;
+    }
+    s.mask = mask;
+    s.keep = mask != 0;
+  }
+  return s;
+}
+
+struct QuartetCounters {
+  unsigned long long quartets = 0, hash = 0, fp32 = 0, prims = 0;
+  __device__ __forceinline__ void add(const Screen& s, const PairD& pb, const PairD& pk, int fp32flag) {
+    quartets += 1;
+    hash += quartet_key(s.i, s.j, s.k, s.l, s.mask);
+    if (fp32flag) fp32 += 1;
+    prims += (unsigned long long)pb.nprim * (unsigned long long)pk.nprim;
+  }
+  __device__ __forceinline__ void flush(Counters* c) {
+    unsigned long long q = warp_sum_u64(quartets), h = warp_sum_u64(hash), f = warp_sum_u64(fp32),
+                       p = warp_sum_u64(prims);
+    if ((threadIdx.x & 31) == 0 && c) {
+      if (q) atomicAdd(&c->quartets, q);
+      if (h) atomicAdd(&c->hash, h);
+      if (f) atomicAdd(&c->fp32_quartets, f);
+      if (p) atomicAdd(&c->prim_quartets, p);
+    }
+  }
+};
+
+// ------------------------------------------------------- horizontal recurrences
+
+// Bra HRR (a, b+1_i | f) = (a+1_i, b | f) + AB_i (a, b | f), i = first
+// nonzero axis of b (src/engine/os_eri.rs:3083-3116), level by level over the
+// whole table; returns the buffer that holds [b][a][f] with a of degree la.
+__device__ __forceinline__ double* hrr_bra(double* buf[3], int& cur, int la, int lb, int nfp, const double ab[3],
+                                           int lane, int T, unsigned tmask) {
+  const int ne = la + lb;
+  const int base_a = tri_below(la);
+  for (int kb = 1; kb <= lb; ++kb) {
+    const double* src = buf[cur];
+    double* dst = buf[(cur + 1) % 3];
+    const int nb_k = ncart(kb);
+    const int na_k = nrange(la, ne - kb);
+    const int na_p = nrange(la, ne - kb + 1);
+    const int total = nb_k * na_k * nfp;
+    for (int q = lane; q < total; q += T) {
+      const int f = q % nfp;
+      const int r = q / nfp;
+      const int ia = r % na_k;
+      const int ib = r / na_k;
+      // b: component ib of degree kb
+      const int baddr = tri_below(kb) + ib;
+      const int bx = addr_lx(baddr), by = addr_ly(baddr), bz = addr_lz(baddr);
+      const int ax_ = bx > 0 ? 0 : (by > 0 ? 1 : 2);
+      const int b1x = bx - (ax_ == 0), b1y = by - (ax_ == 1), b1z = bz - (ax_ == 2);
+      const int ib1 = cart_index3(b1x, b1y, b1z);
+      const int aaddr = base_a + ia;
+      const int ax = addr_lx(aaddr), ay = addr_ly(aaddr), az = addr_lz(aaddr);
+      const int ia1 = addr3(ax + (ax_ == 0), ay + (ax_ == 1), az + (ax_ == 2)) - base_a;
+      const double v1 = src[((size_t)ib1 * na_p + ia1) * nfp + f];
+      const double v0 = src[((size_t)ib1 * na_p + ia) * nfp + f];
+      dst[q] = v1 + ab[ax_] * v0;
+    }
+    __syncwarp(tmask);
+    cur = (cur + 1) % 3;
+  }
+  return buf[cur];
+}
+
+// Ket HRR per (a,b) row, then the Cartesian block [a][b][c][d].
+__device__ __forceinline__ void hrr_ket(double* buf[3], int hcur, double* blk, int la, int lb, int lc, int ld,
+                                        int nfp, const double cd[3], int lane, int T, unsigned tmask) {
+  const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
+  const int nab = na * nb;
+  const int nf = lc + ld;
+  const int base_c = tri_below(lc);
+  const double* H = buf[hcur];  // [ib][ia][f]
+  if (ld == 0) {
+    const int total = nab * nc;
+    for (int q = lane; q < total; q += T) {
+      const int ic = q % nc, ab = q / nc;
+      const int ia = ab / nb, ib = ab % nb;
+      blk[q] = H[((size_t)ib * na + ia) * nfp + ic];
+    }
+    __syncwarp(tmask);
+    return;
+  }
+  int cur = -1;  // level 0 read from H
+  int w0 = (hcur + 1) % 3, w1 = (hcur + 2) % 3;
+  const double* src = H;
+  for (int kd = 1; kd <= ld; ++kd) {
+    double* dst = (kd & 1) ? buf[w0] : buf[w1];
+    const int nd_k = ncart(kd);
+    const int nc_k = nrange(lc, nf - kd);
+    const int nc_p = nrange(lc, nf - kd + 1);
+    const int total = nab * nd_k * nc_k;
+    for (int q = lane; q < total; q += T) {
+      const int ic = q % nc_k;
+      const int r = q / nc_k;
+      const int id = r % nd_k;
+      const int ab = r / nd_k;
+      const int daddr = tri_below(kd) + id;
+      const int dx = addr_lx(daddr), dy = addr_ly(daddr), dz = addr_lz(daddr);
+      const int jx = dx > 0 ? 0 : (dy > 0 ? 1 : 2);
+      const int id1 = cart_index3(dx - (jx == 0), dy - (jx == 1), dz - (jx == 2));
+      const int caddr = base_c + ic;
+      const int cx = addr_lx(caddr), cy = addr_ly(caddr), cz = addr_lz(caddr);
+      const int ic1 = addr3(cx + (jx == 0), cy + (jx == 1), cz + (jx == 2)) - base_c;
+      double v1, v0;
+      if (kd == 1) {
+        const int ia = ab / nb, ib = ab % nb;
+        const size_t row = ((size_t)ib * na + ia) * nfp;
+        v1 = src[row + ic1];
+        v0 = src[row + ic];
+      } else {
+        v1 = src[((size_t)ab * ncart(kd - 1) + id1) * nc_p + ic1];
+        v0 = src[((size_t)ab * ncart(kd - 1) + id1) * nc_p + ic];
+      }
+      dst[q] = v1 + cd[jx] * v0;
+    }
+    __syncwarp(tmask);
+    src = dst;
+    (void)cur;
+  }
+  // final level [ab][d][c] (c of degree lc) -> block [ab][c][d]
+  const int total = nab * nc * nd;
+  for (int q = lane; q < total; q += T) {
+    const int id = q % nd;
+    const int r = q / nd;
+    const int ic = r % nc;
+    const int ab = r / nc;
+    blk[q] = src[((size_t)ab * nd + id) * nc + ic];
+  }
+  __syncwarp(tmask);
+}
+
+// Apply the per-axis c2s matrix (nfunc x ncart) of every spherical shell
+// (src/spherical.rs:121-179); dims updated in place.  Returns the buffer that
+// holds the function-space block.
+__device__ __forceinline__ double* c2s_block(const KernelArgs& A, double* blk, double* tmp, int dims[4],
+                                             const int ls[4], const int sph[4], int lane, int T,
+                                             unsigned tmask) {
+  double* cur = blk;
+  double* oth = tmp;
+  for (int axis = 0; axis < 4; ++axis) {
+    if (!sph[axis]) continue;
+    const int l = ls[axis];
+    const int n_in = dims[axis], n_out = 2 * l + 1;
+    const double* M = A.c2s + A.c2s_off[l];
+    int outer = 1, inner = 1;
+    for (int q = 0; q < axis; ++q) outer *= dims[q];
+    for (int q = axis + 1; q < 4; ++q) inner *= dims[q];
+    const int total = outer * n_out * inner;
+    for (int q = lane; q < total; q += T) {
+      const int s = q % inner;
+      const int r = q / inner;
+      const int o = r / n_out, m = r % n_out;
+      double acc = 0.0;
+      for (int j = 0; j < n_in; ++j) {
+        const double c = __ldg(M + m * n_in + j);
+        if (c != 0.0) acc += c * cur[((size_t)o * n_in + j) * inner + s];
+      }
+      oth[q] = acc;
+    }
+    __syncwarp(tmask);
+    dims[axis] = n_out;
+    double* t = cur;
+    cur = oth;
+    oth = t;
+  }
+  return cur;
+}
+
+// ----------------------------------------------------------------- consumers
+
+// Shell tuples of the 8 permutations (src/integrals.rs:1235-1244) and which
+// of them are distinct (the reference's dedup by permuted shell tuple).
+__device__ __forceinline__ unsigned distinct_perms(const int s[4]) {
+  const int P[8][4] = {{0, 1, 2, 3}, {1, 0, 2, 3}, {0, 1, 3, 2}, {1, 0, 3, 2},
+                       {2, 3, 0, 1}, {2, 3, 1, 0}, {3, 2, 0, 1}, {3, 2, 1, 0}};
+  unsigned w = 0;
+  for (int p = 0; p < 8; ++p) {
+    bool dup = false;
+    for (int q = 0; q < p; ++q)
+      if ((w >> q) & 1u)
+        if (s[P[p][0]] == s[P[q][0]] && s[P[p][1]] == s[P[q][1]] && s[P[p][2]] == s[P[q][2]] &&
+            s[P[p][3]] == s[P[q][3]])
+          dup = true;
+    if (!dup) w |= 1u << p;
+  }
+  return w;
+}
+
+// One contraction term: for every (iu, iv) on axes (u, v) of the block,
+// val = sum over axes (s, t) of B * Dm[row axis ds][col axis dt]; then
+// T1[u-row][v-col] += w1*val and T2[v-row][u-col] += w2*val.
+__device__ __forceinline__ void jk_term(const double* B, const int dims[4], const int offs[4], int nao, int u, int v,
+                                        int s, int t, const double* Dm, int ds, int dt, double* T1, double w1,
+                                        double* T2, double w2, int lane, int T) {
+  const int st[4] = {dims[1] * dims[2] * dims[3], dims[2] * dims[3], dims[3], 1};
+  const int nu = dims[u], nv = dims[v], ns = dims[s], nt = dims[t];
+  for (int q = lane; q < nu * nv; q += T) {
+    const int iu = q / nv, iv = q % nv;
+    const size_t bb = (size_t)iu * st[u] + (size_t)iv * st[v];
+    double acc = 0.0;
+    for (int is = 0; is < ns; ++is) {
+      for (int it = 0; it < nt; ++it) {
+        const int ids = ds == s ? is : it;
+        const int idt = dt == s ? is : it;
+        const double dv = __ldg(Dm + (size_t)(offs[ds] + ids) * nao + offs[dt] + idt);
+        acc += B[bb + (size_t)is * st[s] + (size_t)it * st[t]] * dv;
+      }
+    }
+    if (w1 != 0.0) atomicAdd(T1 + (size_t)(offs[u] + iu) * nao + offs[v] + iv, w1 * acc);
+    if (w2 != 0.0) atomicAdd(T2 + (size_t)(offs[v] + iv) * nao + offs[u] + iu, w2 * acc);
+  }
+}
+
+__device__ __forceinline__ void consume_jk(const KernelArgs& A, const double* B, const int dims[4],
+                                           const int offs[4], const int sh[4], uint64_t mask, int lane, int T) {
+  const unsigned w = distinct_perms(sh);
+  auto W = [&](int p) { return (double)((w >> p) & 1u); };
+  const int nao = A.nao;
+  const size_t n2 = (size_t)nao * nao;
+  for (int d = 0; d < A.jk.ndens; ++d) {
+    if (!((mask >> d) & 1ull)) continue;
+    const double* Dm = A.jk.D + d * n2;
+    double* J = A.jk.J + d * n2;
+    double* K = A.jk.want_k ? A.jk.K + d * n2 : nullptr;
+    if (A.jk.symmetric) {
+      jk_term(B, dims, offs, nao, 0, 1, 2, 3, Dm, 2, 3, J, W(0) + W(2), J, W(1) + W(3), lane, T);
+      jk_term(B, dims, offs, nao, 2, 3, 0, 1, Dm, 0, 1, J, W(4) + W(5), J, W(6) + W(7), lane, T);
+      if (K) {
+        jk_term(B, dims, offs, nao, 0, 2, 1, 3, Dm, 1, 3, K, W(0), K, W(4), lane, T);
+        jk_term(B, dims, offs, nao, 1, 2, 0, 3, Dm, 0, 3, K, W(1), K, W(5), lane, T);
+        jk_term(B, dims, offs, nao, 0, 3, 1, 2, Dm, 1, 2, K, W(2), K, W(6), lane, T);
+        jk_term(B, dims, offs, nao, 1, 3, 0, 2, Dm, 0, 2, K, W(3), K, W(7), lane, T);
+      }
+    } else {
+      // P0..P3 J on (A,B); P4..P7 J on (C,D)
+      jk_term(B, dims, offs, nao, 0, 1, 2, 3, Dm, 2, 3, J, W(0), J, W(1), lane, T);
+      jk_term(B, dims, offs, nao, 0, 1, 2, 3, Dm, 3, 2, J, W(2), J, W(3), lane, T);
+      jk_term(B, dims, offs, nao, 2, 3, 0, 1, Dm, 0, 1, J, W(4), J, W(6), lane, T);
+      jk_term(B, dims, offs, nao, 2, 3, 0, 1, Dm, 1, 0, J, W(5), J, W(7), lane, T);
+      if (K) {
+        jk_term(B, dims, offs, nao, 0, 2, 1, 3, Dm, 1, 3, K, W(0), K, 0.0, lane, T);
+        jk_term(B, dims, offs, nao, 0, 2, 1, 3, Dm, 3, 1, K, 0.0, K, W(4), lane, T);
+        jk_term(B, dims, offs, nao, 1, 2, 0, 3, Dm, 0, 3, K, W(1), K, 0.0, lane, T);
+        jk_term(B, dims, offs, nao, 1, 2, 0, 3, Dm, 3, 0, K, 0.0, K, W(5), lane, T);
+        jk_term(B, dims, offs, nao, 0, 3, 1, 2, Dm, 1, 2, K, W(2), K, 0.0, lane, T);
+        jk_term(B, dims, offs, nao, 0, 3, 1, 2, Dm, 2, 1, K, 0.0, K, W(6), lane, T);
+        jk_term(B, dims, offs, nao, 1, 3, 0, 2, Dm, 0, 2, K, W(3), K, 0.0, lane, T);
+        jk_term(B, dims, offs, nao, 1, 3, 0, 2, Dm, 2, 0, K, 0.0, K, W(7), lane, T);
+      }
+    }
+  }
+}
+
+// Dense tensor: every distinct permutation slot of the block, written once
+// (src/integrals.rs:1271-1312).
+__device__ __forceinline__ void consume_dense(const KernelArgs& A, const double* B, const int dims[4],
+                                              const int offs[4], const int sh[4], int lane, int T) {
+  const int P[8][4] = {{0, 1, 2, 3}, {1, 0, 2, 3}, {0, 1, 3, 2}, {1, 0, 3, 2},
+                       {2, 3, 0, 1}, {2, 3, 1, 0}, {3, 2, 0, 1}, {3, 2, 1, 0}};
+  const unsigned w = distinct_perms(sh);
+  const size_t n = (size_t)A.nao;
+  const int total = dims[0] * dims[1] * dims[2] * dims[3];
+  for (int q = lane; q < total; q += T) {
+    int idx[4];
+    idx[3] = q % dims[3];
+    int r = q / dims[3];
+    idx[2] = r % dims[2];
+    r /= dims[2];
+    idx[1] = r % dims[1];
+    idx[0] = r / dims[1];
+    size_t X[4];
+    for (int a = 0; a < 4; ++a) X[a] = (size_t)(offs[a] + idx[a]);
+    const double v = B[q];
+    for (int p = 0; p < 8; ++p) {
+      if (!((w >> p) & 1u)) continue;
+      A.dense[((X[P[p][0]] * n + X[P[p][1]]) * n + X[P[p][2]]) * n + X[P[p][3]]] = v;
+    }
+  }
+}
+
+// EriBuilder fill: the four bra/ket-internal slots of the requested bra pair
+// (src/eri_builder.rs:650-690).  `bra_is_eval_ket` tells which evaluation
+// pair is the requested bra.
+__device__ __forceinline__ void consume_builder(const KernelArgs& A, const double* B, const int dims[4],
+                                                const int offs[4], const int sh[4], bool bra_is_eval_ket,
+                                                int lane, int T) {
+  const size_t n = (size_t)A.nao;
+  const int total = dims[0] * dims[1] * dims[2] * dims[3];
+  const int r0 = bra_is_eval_ket ? 2 : 0, r1 = bra_is_eval_ket ? 3 : 1;
+  const int c0 = bra_is_eval_ket ? 0 : 2, c1 = bra_is_eval_ket ? 1 : 3;
+  const bool bra_same = sh[r0] == sh[r1];
+  const bool ket_same = sh[c0] == sh[c1];
+  for (int q = lane; q < total; q += T) {
+    int idx[4];
+    idx[3] = q % dims[3];
+    int r = q / dims[3];
+    idx[2] = r % dims[2];
+    r /= dims[2];
+    idx[1] = r % dims[1];
+    idx[0] = r / dims[1];
+    size_t X[4];
+    for (int a = 0; a < 4; ++a) X[a] = (size_t)(offs[a] + idx[a]);
+    const double v = B[q];
+    const size_t mu = X[r0], nu = X[r1], la = X[c0], sg = X[c1];
+    A.dense[((mu * n + nu) * n + la) * n + sg] = v;
+    if (!bra_same) A.dense[((nu * n + mu) * n + la) * n + sg] = v;
+    if (!ket_same) A.dense[((mu * n + nu) * n + sg) * n + la] = v;
+    if (!bra_same && !ket_same) A.dense[((nu * n + mu) * n + sg) * n + la] = v;
+  }
+}
+
+// Schwarz: sqrt(max |(mu nu|mu nu)|) over the function-space diagonal of the
+// (ij|ij) block (src/integrals.rs:850-860).
+__device__ __forceinline__ void consume_schwarz(const KernelArgs& A, const double* B, const int dims[4],
+                                                int pair_index, int lane, int T, unsigned tmask) {
+  const int ni = dims[0], nj = dims[1];
+  double mx = 0.0;
+  for (int q = lane; q < ni * nj; q += T) {
+    const int mu = q / nj, nu = q % nj;
+    mx = fmax(mx, fabs(B[(((size_t)mu * nj + nu) * ni + mu) * nj + nu]));
+  }
+  for (int o = T / 2; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(tmask, mx, o, T));
+  if (lane == 0) A.schwarz_out[pair_index] = sqrt(mx);
+}
+
+// Post phase of one quartet: G (in slot) -> Cartesian block -> function
+// block -> consumer.
+__device__ __forceinline__ void post_quartet(const KernelArgs& A, const ClassDims& cd_, const PairD& pb,
+                                             const PairD& pk, const Screen& sc, double* slot, int lane, int T,
+                                             unsigned tmask, int pb_index) {
+  const int la = cd_.la, lb = cd_.lb, lc = cd_.lc, ld = cd_.ld;
+  const SlotLayout L = slot_layout(la, lb, lc, ld);
+  double* buf[3] = {slot, slot + L.S, slot + 2 * L.S};
+  double* blk = slot + 3 * L.S;
+  double* tmp = blk + L.blk;
+  const int nfp = nrange(lc, lc + ld);
+  const double ab[3] = {pb.abx, pb.aby, pb.abz};
+  const double cdv[3] = {pk.abx, pk.aby, pk.abz};
+  int cur = 0;
+  hrr_bra(buf, cur, la, lb, nfp, ab, lane, T, tmask);
+  hrr_ket(buf, cur, blk, la, lb, lc, ld, nfp, cdv, lane, T, tmask);
+  const int shl[4] = {pb.a, pb.b, pk.a, pk.b};
+  const DevShell s0 = A.shells[shl[0]], s1 = A.shells[shl[1]], s2 = A.shells[shl[2]], s3 = A.shells[shl[3]];
+  int dims[4] = {ncart(la), ncart(lb), ncart(lc), ncart(ld)};
+  const int ls[4] = {la, lb, lc, ld};
+  const int sph[4] = {s0.spherical, s1.spherical, s2.spherical, s3.spherical};
+  const double* B = c2s_block(A, blk, tmp, dims, ls, sph, lane, T, tmask);
+  const int offs[4] = {s0.off, s1.off, s2.off, s3.off};
+  switch (A.mode) {
+    case MODE_JK:
+      consume_jk(A, B, dims, offs, shl, sc.mask, lane, T);
+      break;
+    case MODE_DENSE:
+      consume_dense(A, B, dims, offs, shl, lane, T);
+      break;
+    case MODE_BUILDER:
+      consume_builder(A, B, dims, offs, shl, A.builder_swap != 0, lane, T);
+      break;
+    case MODE_SCHWARZ:
+      consume_schwarz(A, B, dims, pb_index, lane, T, tmask);
+      break;
+    default:
+      break;
+  }
+}
+
+}  // namespace igpu

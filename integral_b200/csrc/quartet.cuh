@@ -1,0 +1,293 @@
+// Shell-quartet kernels of the two-electron path.
+//
+// One launch handles one angular class (la,lb|lc,ld) in evaluation
+// orientation (la >= lb, lc >= ld, bra class >= ket class) over a task list
+// of (bra pair, ket pair) quartets that survived the Schwarz product screen.
+//
+// Phase 1 builds the contracted table G[e][f] = sum over primitive quartets
+// and Rys roots of Ix[ex][fx] Iy[ey][fy] Iz[ez][fz] (the [e0|f0] integrals,
+// e of degree la..la+lb on A, f of degree lc..lc+ld on C) by Rys quadrature
+// with the vertical recurrence of src/engine/rys.rs:234-268.  Doing the
+// horizontal recurrence once per shell quartet on the contracted table is the
+// early-contraction scheme of the reference's OS/HGP engine
+// (src/engine/os_eri.rs:1-12) applied to Rys 2D integrals.
+//   TEAM == 1 : one thread per quartet, everything in registers.
+//   TEAM >= 8 : a team of TEAM lanes per quartet; roots and the 3*nroots
+//               per-axis tables are built cooperatively in shared memory and
+//               every lane accumulates its own rows e of G (register tiles
+//               of FCH columns, the f range walked in chunks).
+// Phase 2 (post.cuh) runs the horizontal recurrences, the Cartesian ->
+// spherical transform and the mode-specific consumer on the team.
+#pragma once
+#include "device_common.cuh"
+#include "post.cuh"
+
+namespace igpu {
+
+template <int LA, int LB, int LC, int LD>
+struct ClassShape {
+  static constexpr int NE = LA + LB;
+  static constexpr int NF = LC + LD;
+  static constexpr int LT = NE + NF;
+  static constexpr int NR = LT / 2 + 1;
+  static constexpr int NEP = nrange(LA, NE);
+  static constexpr int NFP = nrange(LC, NF);
+  static constexpr int NG = NEP * NFP;
+};
+
+// Team size per class: one thread while the whole G table fits comfortably
+// in registers, otherwise the smallest power-of-two team covering the rows.
+template <int LA, int LB, int LC, int LD>
+__host__ __device__ constexpr int team_size() {
+  constexpr int nep = nrange(LA, LA + LB), nfp = nrange(LC, LC + LD);
+  if (nep * nfp <= 81) return 1;
+  if (nep <= 8) return 8;
+  if (nep <= 16) return 16;
+  return 32;
+}
+
+// Phase-1 register footprint per lane: rows x FCH accumulators.
+template <typename R>
+__host__ __device__ constexpr int max_acc() { return sizeof(R) == 8 ? 64 : 96; }
+
+template <int LA, int LB, int LC, int LD, typename R>
+struct TeamShape {
+  using S = ClassShape<LA, LB, LC, LD>;
+  static constexpr int T = team_size<LA, LB, LC, LD>();
+  static constexpr int ROWS = (S::NEP + T - 1) / T;
+  static constexpr int FCH0 = max_acc<R>() / ROWS;
+  static constexpr int FCH = FCH0 < 1 ? 1 : (FCH0 > S::NFP ? S::NFP : FCH0);
+  static constexpr int NCHUNK = (S::NFP + FCH - 1) / FCH;
+  // shared memory per team and buffer: x[NR], w[NR], g[3][NR][NE+1][NF+1]
+  static constexpr int GTAB = (S::NE + 1) * (S::NF + 1);
+  static constexpr int BUF = 2 * S::NR + 3 * S::NR * GTAB;
+  static constexpr int SMEM_PER_TEAM = T == 1 ? 0 : 2 * BUF;  // in R units
+};
+
+// ------------------------------------------------------------- TEAM == 1
+
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void accumulate_thread(const KernelArgs& A, const PairD& pb, const PairD& pk,
+                                                  R (&G)[ClassShape<LA, LB, LC, LD>::NG]) {
+  using S = ClassShape<LA, LB, LC, LD>;
+  constexpr int NE = S::NE, NF = S::NF, NR = S::NR;
+#pragma unroll
+  for (int q = 0; q < S::NG; ++q) G[q] = R(0);
+  for (int ip = 0; ip < pb.nprim; ++ip) {
+    const PrimPairD bp = A.prims[pb.prim_off + ip];
+    for (int kq = 0; kq < pk.nprim; ++kq) {
+      const PrimPairD kp = A.prims[pk.prim_off + kq];
+      const QuartetHdr<R> h = quartet_header<R>(bp, kp);
+      R x[NR], w[NR];
+      rys_roots<NR, R>(h.T, x, w);
+      const R inv_pq = R(1) / h.pq;
+      const R qpq = h.q * inv_pq, ppq = h.p * inv_pq;
+      const R inv2pq = R(0.5) * inv_pq, inv2p = R(0.5) / h.p, inv2q = R(0.5) / h.q;
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const R xr = x[r];
+        const R b00 = xr * inv2pq;
+        const R b10 = (R(1) - xr * qpq) * inv2p;
+        const R b01 = (R(1) - xr * ppq) * inv2q;
+        const R cq = xr * qpq, cp = xr * ppq;
+        R gx[NE + 1][NF + 1], gy[NE + 1][NF + 1], gz[NE + 1][NF + 1];
+        vrr_axis<NE, NF, R>(R(1), h.pax - cq * h.pqx, h.qcx + cp * h.pqx, b10, b01, b00, gx);
+        vrr_axis<NE, NF, R>(R(1), h.pay - cq * h.pqy, h.qcy + cp * h.pqy, b10, b01, b00, gy);
+        vrr_axis<NE, NF, R>(w[r] * h.pref, h.paz - cq * h.pqz, h.qcz + cp * h.pqz, b10, b01, b00, gz);
+        static_for<S::NEP>([&](auto e) {
+          constexpr int ex = range_x(LA, decltype(e)::value);
+          constexpr int ey = range_y(LA, decltype(e)::value);
+          constexpr int ez = range_z(LA, decltype(e)::value);
+          static_for<S::NFP>([&](auto f) {
+            constexpr int fx = range_x(LC, decltype(f)::value);
+            constexpr int fy = range_y(LC, decltype(f)::value);
+            constexpr int fz = range_z(LC, decltype(f)::value);
+            G[decltype(e)::value * S::NFP + decltype(f)::value] += gx[ex][fx] * gy[ey][fy] * gz[ez][fz];
+          });
+        });
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------- TEAM > 1
+
+// Root r of the N-point quadrature (one lane per root).
+template <int N, typename R>
+__device__ __forceinline__ void rys_root_one(R T, int r, R& x, R& w) {
+  const RysMeta m = c_rys[N];
+  if (T >= R(m.t_hi)) {
+    if constexpr (sizeof(R) == 8) {
+      x = c_lag_x[N - 1][r] / T;
+      w = c_lag_w[N - 1][r] * R(0.5) * rsqrt(T);
+    } else {
+      x = c_lag_xf[N - 1][r] / T;
+      w = c_lag_wf[N - 1][r] * R(0.5) * rsqrt(T);
+    }
+    return;
+  }
+  R width = R(m.width);
+  int s = (int)(T / width);
+  s = s < 0 ? 0 : (s >= m.n_sub ? m.n_sub - 1 : s);
+  R a = R(s) * width;
+  R b = a + width;
+  R xi = (R(2) * T - (a + b)) / (b - a);
+  const R* base;
+  if constexpr (sizeof(R) == 8)
+    base = c_rys_tab + m.off + ((size_t)s * N + r) * 2 * RYS_NC;
+  else
+    base = c_rys_tab_f + m.off + ((size_t)s * N + r) * 2 * RYS_NC;
+  x = chebev<R>(base, xi);
+  w = chebev<R>(base + RYS_NC, xi);
+}
+
+// One pass over all primitive quartets accumulating the columns
+// [F0, F0 + FCH) of this lane's rows.
+template <int LA, int LB, int LC, int LD, typename R, int F0>
+__device__ __forceinline__ void team_pass(const KernelArgs& A, const PairD& pb, const PairD& pk, R* sm,
+                                          int lane, unsigned tmask, double* G) {
+  using S = ClassShape<LA, LB, LC, LD>;
+  using TS = TeamShape<LA, LB, LC, LD, R>;
+  constexpr int NE = S::NE, NF = S::NF, NR = S::NR, T = TS::T;
+  constexpr int FW = (F0 + TS::FCH <= S::NFP) ? TS::FCH : (S::NFP - F0);
+  constexpr int GT = TS::GTAB;
+  R acc[TS::ROWS][FW];
+#pragma unroll
+  for (int k = 0; k < TS::ROWS; ++k)
+#pragma unroll
+    for (int f = 0; f < FW; ++f) acc[k][f] = R(0);
+  int ex[TS::ROWS], ey[TS::ROWS], ez[TS::ROWS];
+#pragma unroll
+  for (int k = 0; k < TS::ROWS; ++k) {
+    int e = lane + T * k;
+    int a = tri_below(LA) + (e < S::NEP ? e : 0);
+    ex[k] = addr_lx(a);
+    ey[k] = addr_ly(a);
+    ez[k] = addr_lz(a);
+  }
+  int buf = 0;
+  for (int ip = 0; ip < pb.nprim; ++ip) {
+    const PrimPairD bp = A.prims[pb.prim_off + ip];
+    for (int kq = 0; kq < pk.nprim; ++kq) {
+      const PrimPairD kp = A.prims[pk.prim_off + kq];
+      const QuartetHdr<R> h = quartet_header<R>(bp, kp);
+      R* B = sm + buf * TS::BUF;
+      R* xs = B;
+      R* ws = B + NR;
+      R* gt = B + 2 * NR;
+      if (lane < NR) {
+        R xr, wr;
+        rys_root_one<NR, R>(h.T, lane, xr, wr);
+        xs[lane] = xr;
+        ws[lane] = wr * h.pref;
+      }
+      __syncwarp(tmask);
+      if (lane < 3 * NR) {
+        const int axis = lane / NR, r = lane - axis * NR;
+        const R inv_pq = R(1) / h.pq;
+        const R xr = xs[r];
+        const R qpq = h.q * inv_pq, ppq = h.p * inv_pq;
+        const R b00 = xr * R(0.5) * inv_pq;
+        const R b10 = (R(1) - xr * qpq) * (R(0.5) / h.p);
+        const R b01 = (R(1) - xr * ppq) * (R(0.5) / h.q);
+        const R pqa = axis == 0 ? h.pqx : (axis == 1 ? h.pqy : h.pqz);
+        const R paa = axis == 0 ? h.pax : (axis == 1 ? h.pay : h.paz);
+        const R qca = axis == 0 ? h.qcx : (axis == 1 ? h.qcy : h.qcz);
+        R g[NE + 1][NF + 1];
+        vrr_axis<NE, NF, R>(axis == 2 ? ws[r] : R(1), paa - xr * qpq * pqa, qca + xr * ppq * pqa, b10, b01,
+                            b00, g);
+        R* dst = gt + (axis * NR + r) * GT;
+#pragma unroll
+        for (int n = 0; n <= NE; ++n)
+#pragma unroll
+          for (int m = 0; m <= NF; ++m) dst[n * (NF + 1) + m] = g[n][m];
+      }
+      __syncwarp(tmask);
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const R* tx = gt + (0 * NR + r) * GT;
+        const R* ty = gt + (1 * NR + r) * GT;
+        const R* tz = gt + (2 * NR + r) * GT;
+#pragma unroll
+        for (int k = 0; k < TS::ROWS; ++k) {
+          if (TS::ROWS * T > S::NEP && lane + T * k >= S::NEP) continue;
+          R rx[NF + 1], ry[NF + 1], rz[NF + 1];
+#pragma unroll
+          for (int m = 0; m <= NF; ++m) {
+            rx[m] = tx[ex[k] * (NF + 1) + m];
+            ry[m] = ty[ey[k] * (NF + 1) + m];
+            rz[m] = tz[ez[k] * (NF + 1) + m];
+          }
+          static_for<FW>([&](auto f) {
+            constexpr int fi = F0 + decltype(f)::value;
+            constexpr int fx = range_x(LC, fi), fy = range_y(LC, fi), fz = range_z(LC, fi);
+            acc[k][decltype(f)::value] += rx[fx] * ry[fy] * rz[fz];
+          });
+        }
+      }
+      buf ^= 1;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < TS::ROWS; ++k) {
+    int e = lane + T * k;
+    if (e < S::NEP) {
+#pragma unroll
+      for (int f = 0; f < FW; ++f) G[(size_t)e * S::NFP + F0 + f] = (double)acc[k][f];
+    }
+  }
+}
+
+template <int LA, int LB, int LC, int LD, typename R, int C>
+__device__ __forceinline__ void team_chunks(const KernelArgs& A, const PairD& pb, const PairD& pk, R* sm,
+                                            int lane, unsigned tmask, double* G) {
+  using TS = TeamShape<LA, LB, LC, LD, R>;
+  if constexpr (C < TS::NCHUNK) {
+    team_pass<LA, LB, LC, LD, R, C * TS::FCH>(A, pb, pk, sm, lane, tmask, G);
+    __syncwarp(tmask);
+    team_chunks<LA, LB, LC, LD, R, C + 1>(A, pb, pk, sm, lane, tmask, G);
+  }
+}
+
+// ------------------------------------------------------------------ kernel
+
+template <int LA, int LB, int LC, int LD, typename R>
+__global__ void __launch_bounds__(128) quartet_kernel(KernelArgs A) {
+  using S = ClassShape<LA, LB, LC, LD>;
+  using TS = TeamShape<LA, LB, LC, LD, R>;
+  constexpr int T = TS::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int team = tid / T;
+  const int lane = threadIdx.x % T;
+  const int nteams = (gridDim.x * blockDim.x) / T;
+  const unsigned tmask = T == 32 ? 0xffffffffu : (((1u << T) - 1u) << ((threadIdx.x % 32) / T * T));
+  R* sm = reinterpret_cast<R*>(smem_raw) + (size_t)(threadIdx.x / T) * TS::SMEM_PER_TEAM;
+  double* slot = A.scratch + (size_t)team * A.slot_doubles;
+  QuartetCounters cnt;
+  const ClassDims dims{LA, LB, LC, LD};
+
+  for (unsigned long long g = team; g < A.task.total; g += nteams) {
+    int pbi, pki;
+    decode_task(A.task, g, pbi, pki);
+    const PairD pb = A.pairs[pbi];
+    const PairD pk = A.pairs[pki];
+    Screen sc = screen_quartet(A, pb, pk);
+    if (!sc.keep) continue;
+    if (lane == 0) cnt.add(sc, pb, pk, A.fp32);
+    if constexpr (T == 1) {
+      R G[S::NG];
+      accumulate_thread<LA, LB, LC, LD, R>(A, pb, pk, G);
+#pragma unroll
+      for (int q = 0; q < S::NG; ++q) slot[q] = (double)G[q];
+    } else {
+      team_chunks<LA, LB, LC, LD, R, 0>(A, pb, pk, sm, lane, tmask, slot);
+    }
+    __syncwarp(tmask);
+    post_quartet(A, dims, pb, pk, sc, slot, lane, T, tmask, pbi);
+    __syncwarp(tmask);
+  }
+  cnt.flush(A.counters);
+}
+
+}  // namespace igpu
