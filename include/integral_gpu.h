@@ -94,6 +94,19 @@ typedef struct {
   uint32_t launches;          /* kernels launched by the call */
 } igpu_stats;
 
+/* One quartet-kernel launch of the last J/K or gradient call. */
+typedef struct {
+  int la, lb, lc, ld;         /* angular class in evaluation orientation */
+  int fp32;                   /* evaluated in FP32 */
+  int team;                   /* lanes per quartet */
+  uint32_t grid;              /* blocks of 128 threads */
+  uint64_t tasks;             /* quartets in the launch's task list */
+  uint64_t quartets;          /* of them accepted by the screening */
+  uint64_t prim_quartets;
+  double ms;                  /* device time (CUDA events) */
+  double model_flops;         /* fixed Rys flop model of the accepted work */
+} igpu_launch_record;
+
 /* integral-sys `integral_abi_version` (crates/integral-sys/src/lib.rs:21). */
 uint32_t igpu_abi_version(void);
 
@@ -155,6 +168,9 @@ int igpu_grad_device(igpu_plan* plan, const igpu_term* d_coulomb, int ncoul,
 
 /* Counters of the last J/K or gradient call on the plan. */
 int igpu_last_stats(const igpu_plan* plan, igpu_stats* stats);
+/* Per-launch records of the last J/K or gradient call (*n = count; at most
+ * cap written to out). */
+int igpu_last_profile(const igpu_plan* plan, igpu_launch_record* out, size_t cap, size_t* n);
 
 #ifdef __cplusplus
 }

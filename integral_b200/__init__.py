@@ -168,6 +168,14 @@ class _Plan:
         _lib.check(_lib.lib().igpu_last_stats(self.h, ctypes.byref(st)))
         return {f: getattr(st, f) for f, _ in IgpuStats._fields_}
 
+    def profile(self) -> list:
+        """Per-launch records (class, precision, time, counters) of the last call."""
+        n = ctypes.c_size_t()
+        _lib.check(_lib.lib().igpu_last_profile(self.h, None, 0, ctypes.byref(n)))
+        arr = (_lib.IgpuLaunchRecord * max(1, n.value))()
+        _lib.check(_lib.lib().igpu_last_profile(self.h, arr, n.value, ctypes.byref(n)))
+        return [{f: getattr(arr[k], f) for f, _ in _lib.IgpuLaunchRecord._fields_} for k in range(n.value)]
+
 
 class Basis:
     """An ordered list of shells (src/shell.rs:193-276)."""

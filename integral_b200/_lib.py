@@ -32,6 +32,13 @@ class IgpuStats(ctypes.Structure):
                 ("launches", ctypes.c_uint32)]
 
 
+class IgpuLaunchRecord(ctypes.Structure):
+    _fields_ = [("la", ctypes.c_int), ("lb", ctypes.c_int), ("lc", ctypes.c_int), ("ld", ctypes.c_int),
+                ("fp32", ctypes.c_int), ("team", ctypes.c_int), ("grid", ctypes.c_uint32),
+                ("tasks", ctypes.c_uint64), ("quartets", ctypes.c_uint64), ("prim_quartets", ctypes.c_uint64),
+                ("ms", ctypes.c_double), ("model_flops", ctypes.c_double)]
+
+
 STATUS = {
     0: "ok", -1: "invalid argument", -2: "empty contraction", -3: "mismatched contraction",
     -4: "angular momentum too high", -5: "angular momentum too high for gradient",
@@ -72,6 +79,7 @@ def lib():
     L.igpu_grad_device.argtypes = [vp, ctypes.POINTER(IgpuTerm), ctypes.c_int, ctypes.POINTER(IgpuTerm),
                                    ctypes.c_int, c_u32_p, ctypes.c_size_t, ctypes.c_double, ctypes.c_int, vp, vp]
     L.igpu_last_stats.argtypes = [vp, ctypes.POINTER(IgpuStats)]
+    L.igpu_last_profile.argtypes = [vp, ctypes.POINTER(IgpuLaunchRecord), ctypes.c_size_t, c_size_p]
     _lib = L
     return L
 
@@ -80,7 +88,7 @@ EXPORTED = [
     "igpu_abi_version", "igpu_last_error_string", "igpu_plan_create", "igpu_plan_destroy", "igpu_plan_query",
     "igpu_bra_pairs", "igpu_atoms", "igpu_schwarz", "igpu_set_mixed_cutoff", "igpu_eri_dense",
     "igpu_eri_builder_fill", "igpu_density_shell_bounds", "igpu_jk", "igpu_jk_device", "igpu_grad",
-    "igpu_grad_device", "igpu_last_stats",
+    "igpu_grad_device", "igpu_last_stats", "igpu_last_profile",
 ]
 
 

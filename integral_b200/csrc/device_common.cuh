@@ -133,6 +133,72 @@ __device__ __forceinline__ R chebev(const R* __restrict__ c, R xi) {
   return xi * d - dd + R(0.5) * __ldg(c);
 }
 
+// Largest number of Chebyshev subintervals of any n (15 for n = 13).
+constexpr int RYS_MAX_SUB = 16;
+
+// Copy the N-root table (all subintervals) into shared memory; every thread
+// of the block must call it.  Lookups of different T by the lanes of a warp
+// are then shared-memory reads instead of scattered L1 sectors.
+template <int N, typename R>
+__device__ __forceinline__ void stage_rys_table(R* s_tab) {
+  const RysMeta m = c_rys[N];
+  const R* src;
+  if constexpr (sizeof(R) == 8)
+    src = c_rys_tab + m.off;
+  else
+    src = c_rys_tab_f + m.off;
+  const int sub = m.n_sub < RYS_MAX_SUB ? m.n_sub : RYS_MAX_SUB;
+  const int cnt = sub * N * 2 * RYS_NC;
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) s_tab[i] = __ldg(src + i);
+  __syncthreads();
+}
+
+template <typename R>
+__device__ __forceinline__ R chebev_s(const R* c, R xi) {
+  R two_xi = R(2) * xi;
+  R d = R(0), dd = R(0);
+#pragma unroll
+  for (int k = RYS_NC - 1; k >= 1; --k) {
+    R sv = d;
+    d = two_xi * d - dd + c[k];
+    dd = sv;
+  }
+  return xi * d - dd + R(0.5) * c[0];
+}
+
+// Roots/weights from the shared-memory copy of the N-root table.
+template <int N, typename R>
+__device__ __forceinline__ void rys_roots_s(const R* s_tab, R T, R* x, R* w) {
+  const RysMeta m = c_rys[N];
+  if (T >= R(m.t_hi)) {
+    R inv_t = R(1) / T;
+    R sc = R(0.5) * rsqrt(T);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      if constexpr (sizeof(R) == 8) {
+        x[i] = c_lag_x[N - 1][i] * inv_t;
+        w[i] = c_lag_w[N - 1][i] * sc;
+      } else {
+        x[i] = c_lag_xf[N - 1][i] * inv_t;
+        w[i] = c_lag_wf[N - 1][i] * sc;
+      }
+    }
+    return;
+  }
+  R width = R(m.width);
+  int s = (int)(T / width);
+  s = s < 0 ? 0 : (s >= m.n_sub ? m.n_sub - 1 : s);
+  R a = R(s) * width;
+  R b = a + width;
+  R xi = (R(2) * T - (a + b)) / (b - a);
+  const R* base = s_tab + (size_t)s * N * 2 * RYS_NC;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    x[i] = chebev_s<R>(base + (2 * i) * RYS_NC, xi);
+    w[i] = chebev_s<R>(base + (2 * i + 1) * RYS_NC, xi);
+  }
+}
+
 // N-point Rys quadrature at parameter T (src/math/rys.rs:174-215): the
 // generalized-Laguerre(-1/2) limit above asymptotic_boundary(2N-1), else the
 // piecewise Chebyshev interpolation.  x = squared roots, w = weights.

@@ -99,8 +99,8 @@ enum Mode : int {
 struct JKDev {
   const double* D;       // ndens x nao x nao
   const double* bounds;  // ndens x nsh x nsh  (density_shell_bounds)
-  double* J;
-  double* K;
+  double* J;             // symmetric: one-orientation accumulators J', K'
+  double* K;             //   (J = (J' + J'^T)/2 added by the finalize pass)
   int ndens;
   int want_k;
   int symmetric;         // every density symmetric (bitwise)
@@ -154,6 +154,10 @@ struct KernelArgs {
   Counters* counters;
   int builder_swap;      // builder mode: requested bra is the evaluation ket
   const unsigned* bra_bitmap;  // optional: reference bra pairs to keep (bit per pair)
+  unsigned long long* work_counter;  // next unclaimed task (dynamic chunks)
+  unsigned long long chunk;          // tasks claimed per grab (per warp)
+  size_t acc_offset;     // slot offset of the running bra-block J accumulators
+  int kinds;             // 0 all shells Cartesian, 1 all spherical, 2 mixed
 };
 
 }  // namespace igpu

@@ -134,6 +134,24 @@ cudaError_t launch_shell_block_max(const double* D, int nmat, const DevShell* sh
   return cudaGetLastError();
 }
 
+// out[d] += (H[d] + H[d]^T) / 2: the symmetric J/K from one-orientation
+// accumulators.
+__global__ void symmetrize_add_kernel(const double* __restrict__ H, double* __restrict__ out, int nmat, int nao) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t n2 = (size_t)nao * nao;
+  if (t >= n2 * nmat) return;
+  const size_t d = t / n2, r = (t % n2) / nao, c = t % nao;
+  const double* M = H + d * n2;
+  out[t] += 0.5 * (M[r * nao + c] + M[c * nao + r]);
+}
+
+cudaError_t launch_symmetrize_add(const double* H, double* out, int nmat, int nao, cudaStream_t s) {
+  const size_t n = (size_t)nao * nao * nmat;
+  if (n == 0) return cudaSuccess;
+  symmetrize_add_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(H, out, nmat, nao);
+  return cudaGetLastError();
+}
+
 // flag[0] += 1 for every element with M[r][c] != M[c][r] (bitwise compare).
 __global__ void asym_count_kernel(const double* __restrict__ D, int nmat, int nao, unsigned long long* flag) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;

@@ -31,6 +31,7 @@ cudaError_t launch_quartets(const KernelEntry* e, bool fp32, int grid, const Ker
                             cudaStream_t stream);
 cudaError_t launch_shell_block_max(const double* D, int nmat, const DevShell* sh, int nsh, int nao,
                                    int symmetrise, double* out, cudaStream_t s);
+cudaError_t launch_symmetrize_add(const double* H, double* out, int nmat, int nao, cudaStream_t s);
 cudaError_t launch_asym_count(const double* D, int nmat, int nao, unsigned long long* flag, cudaStream_t s);
 
 }  // namespace igpu

@@ -48,6 +48,11 @@ int cuda_fail(cudaError_t e, const char* where) {
   } while (0)
 
 int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
+int pc_la_host(int pc) {
+  int la = 0;
+  while ((la + 1) * (la + 2) / 2 <= pc) ++la;
+  return la;
+}
 
 template <typename T>
 struct DevBuf {
@@ -103,7 +108,8 @@ struct igpu_plan {
   std::vector<PrimPairD> prims;
   std::vector<double> c2s;
   int c2s_off[GPU_MAX_L + 3] = {0};
-  std::vector<std::vector<int>> class_pairs;  // per pair class, Q-descending
+  std::vector<std::vector<int>> class_pairs;  // per pair class: nprim desc, then Q desc
+  std::vector<std::vector<std::pair<size_t, size_t>>> class_groups;  // equal-nprim runs
   std::vector<double> schwarz;               // nsh x nsh
   // device
   cudaStream_t stream = nullptr;
@@ -118,13 +124,19 @@ struct igpu_plan {
   DevBuf<Counters> d_counters;
   DevBuf<double> d_schwarz_pair;
   // per-call device buffers
-  DevBuf<double> d_D, d_J, d_K, d_bounds, d_dense;
+  DevBuf<double> d_D, d_J, d_K, d_bounds, d_dense, d_Jh, d_Kh;
+  DevBuf<unsigned long long> d_work;
   DevBuf<unsigned long long> d_flag;
   DevBuf<unsigned> d_bitmap;
   std::map<std::pair<double, double>, std::unique_ptr<TaskSet>> jk_tasks;  // (threshold, fp64 cutoff)
   std::unique_ptr<TaskSet> dense_tasks;
   double mixed_cutoff = 1e-4;
+  bool all_spherical = false;
   igpu_stats last{};
+  DevBuf<Counters> d_launch_counters;
+  std::vector<cudaEvent_t> events;
+  std::vector<igpu_launch_record> profile;
+  std::vector<size_t> profile_launch;
   GradState grad;
 };
 
@@ -191,20 +203,87 @@ KernelArgs base_args(igpu_plan* P) {
   A.nsh = P->nsh;
   A.nao = P->nao;
   A.counters = P->d_counters.p;
+  A.kinds = P->all_spherical ? 1 : (P->spherical_any ? 2 : 0);
   return A;
 }
 
-// Run every launch of a task set in `mode`; quartet kernels only.
+// Fixed flop model of the reference's Rys formulation (src/engine/rys.rs:
+// 137-309) per surviving primitive quartet: header, roots/weights by
+// Clenshaw, per root the recurrence coefficients, per axis VRR + bra HRR +
+// ket HRR, and the 4-flop assembly of every Cartesian element.
+double model_flops_prim(int la, int lb, int lc, int ld) {
+  auto nc = [](int l) { return (double)((l + 1) * (l + 2) / 2); };
+  const int n = (la + lb + lc + ld) / 2 + 1, nb = la + lb, nk = lc + ld;
+  const double N4 = nc(la) * nc(lb) * nc(lc) * nc(ld);
+  const double per_root = 12.0 + 3.0 * (3.0 * (nb + 1) * (nk + 1) + 2.0 * lb * (nb + 1) * (nk + 1) +
+                                        2.0 * ld * (la + 1) * (lb + 1) * (nk + 1)) +
+                          4.0 * N4;
+  return 40.0 + 2.0 * n * 34.0 + n * per_root;
+}
+// Per shell quartet: c2s of spherical shells (2 flops per multiply-add of
+// each axis contraction) and the J/K contraction, 4 flops per element and
+// density for each of the 8 permutation images.
+double model_flops_quartet(int la, int lb, int lc, int ld, bool sph, int ndens, bool jk) {
+  auto nc = [](int l) { return (double)((l + 1) * (l + 2) / 2); };
+  double dims[4] = {nc(la), nc(lb), nc(lc), nc(ld)};
+  const int ls[4] = {la, lb, lc, ld};
+  double f = 0.0;
+  if (sph)
+    for (int a = 0; a < 4; ++a) {
+      double rest = 1.0;
+      for (int q = 0; q < 4; ++q)
+        if (q != a) rest *= dims[q];
+      const double out = 2.0 * ls[a] + 1.0;
+      f += 2.0 * out * dims[a] * rest;
+      dims[a] = out;
+    }
+  if (jk) f += 4.0 * 8.0 * dims[0] * dims[1] * dims[2] * dims[3] * ndens;
+  return f;
+}
+
+// Scratch doubles per team: the class slot plus, for symmetric J/K, the
+// running bra-block accumulators (bra index + ndens blocks of the bra pair).
+size_t slot_with_acc(const KernelEntry* e, int pcb, const KernelArgs& A) {
+  if (A.mode != MODE_JK || !A.jk.symmetric) return e->slot;
+  const int la = pc_la_host(pcb), lb = pcb - la * (la + 1) / 2;
+  const size_t nab = (size_t)((la + 1) * (la + 2) / 2) * ((lb + 1) * (lb + 2) / 2);
+  return e->slot + 1 + (size_t)A.jk.ndens * nab;
+}
+
+// Run every launch of a task set; quartet kernels only.  Per-launch device
+// time and counters are kept for igpu_last_profile.
 int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t& launches) {
+  size_t need = 0;
   for (auto& L : ts.launches) {
     if (L->total == 0) continue;
     const KernelEntry* e = kernel_entry(L->pcb, L->pck);
     if (!e) return fail(IGPU_ERR_UNSUPPORTED, "angular class not compiled for the GPU");
+    need = std::max(need, grid_for(e, L->fp32, L->total) * (128 / e->team) * slot_with_acc(e, L->pcb, A));
+  }
+  CK(P->d_scratch.ensure(need));
+  const size_t nl = ts.launches.size();
+  CK(P->d_launch_counters.ensure(nl));
+  CK(cudaMemsetAsync(P->d_launch_counters.p, 0, nl * sizeof(Counters), s));
+  CK(P->d_work.ensure(nl));
+  CK(cudaMemsetAsync(P->d_work.p, 0, nl * sizeof(unsigned long long), s));
+  while (P->events.size() < 2 * nl) {
+    cudaEvent_t ev;
+    CK(cudaEventCreate(&ev));
+    P->events.push_back(ev);
+  }
+  P->profile.clear();
+  P->profile_launch.clear();
+  for (size_t li = 0; li < nl; ++li) {
+    Launch* L = ts.launches[li].get();
+    if (L->total == 0) continue;
+    const KernelEntry* e = kernel_entry(L->pcb, L->pck);
     const size_t grid = grid_for(e, L->fp32, L->total);
-    const size_t teams = grid * (128 / e->team);
-    CK(P->d_scratch.ensure(teams * e->slot));
     A.scratch = P->d_scratch.p;
-    A.slot_doubles = e->slot;
+    A.slot_doubles = slot_with_acc(e, L->pcb, A);
+    A.acc_offset = e->slot;
+    A.work_counter = P->d_work.p + li;
+    A.chunk = (unsigned long long)(32 / e->team) * 16;
+    if (A.counters) A.counters = P->d_launch_counters.p + li;
     A.task.bra_pair = L->bra_pair.p;
     A.task.ket_pairs = L->ket_list;
     A.task.prefix = L->prefix.p;
@@ -213,9 +292,49 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     A.task.total = L->total;
     A.fp32 = L->fp32 ? 1 : 0;
     A.builder_swap = L->builder_swap;
+    CK(cudaEventRecord(P->events[2 * li], s));
     CK(launch_quartets(e, L->fp32, (int)grid, A, s));
+    CK(cudaEventRecord(P->events[2 * li + 1], s));
     ++launches;
+    igpu_launch_record r{};
+    r.la = pc_la_host(L->pcb);
+    r.lb = L->pcb - r.la * (r.la + 1) / 2;
+    r.lc = pc_la_host(L->pck);
+    r.ld = L->pck - r.lc * (r.lc + 1) / 2;
+    r.fp32 = L->fp32 ? 1 : 0;
+    r.team = e->team;
+    r.grid = (uint32_t)grid;
+    r.tasks = L->total;
+    P->profile.push_back(r);
+    P->profile_launch.push_back(li);
   }
+  return IGPU_OK;
+}
+
+// After the stream is synchronised: per-launch times, counters, model flops.
+int collect_profile(igpu_plan* P, int ndens, bool jk) {
+  const size_t nl = P->profile.empty() ? 0 : P->profile_launch.back() + 1;
+  std::vector<Counters> c(nl);
+  if (nl) CK(cudaMemcpy(c.data(), P->d_launch_counters.p, nl * sizeof(Counters), cudaMemcpyDeviceToHost));
+  P->last = igpu_stats{};
+  for (size_t k = 0; k < P->profile.size(); ++k) {
+    igpu_launch_record& r = P->profile[k];
+    const size_t li = P->profile_launch[k];
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, P->events[2 * li], P->events[2 * li + 1]);
+    r.ms = ms;
+    r.quartets = c[li].quartets;
+    r.prim_quartets = c[li].prim_quartets;
+    r.model_flops = (double)r.prim_quartets * model_flops_prim(r.la, r.lb, r.lc, r.ld) +
+                    (double)r.quartets * model_flops_quartet(r.la, r.lb, r.lc, r.ld, P->all_spherical, ndens, jk);
+    P->last.quartets += c[li].quartets;
+    P->last.quartet_hash += c[li].hash;
+    P->last.quartets_fp32 += c[li].fp32_quartets;
+    P->last.prim_quartets += c[li].prim_quartets;
+    P->last.model_flops += r.model_flops;
+    P->last.kernel_ms += ms;
+  }
+  P->last.launches = (uint32_t)P->profile.size();
   return IGPU_OK;
 }
 
@@ -268,40 +387,49 @@ int build_jk_tasks(igpu_plan* P, double tau, double fp64_cut, TaskSet& ts) {
       if (B.empty() || K.empty()) continue;
       std::vector<double> qk(K.size());
       for (size_t x = 0; x < K.size(); ++x) qk[x] = P->pairs[K[x]].q;
-      std::vector<int> bras(B.size()), n64(B.size()), n32(B.size()), st32(B.size());
+      // One segment per (bra, ket group of equal primitive-pair count): the
+      // lanes of a warp then run equal primitive loops.  Within a group the
+      // kets are Q-descending, so the accepted kets are a prefix.
+      const auto& groups = P->class_groups[cb];
+      std::vector<int> bras, n64, n32, st64, st32;
       for (size_t bp = 0; bp < B.size(); ++bp) {
         const double qb = P->pairs[B[bp]].q;
-        // first ket with qb*qk < tau
-        size_t lo = 0, hi = K.size();
-        while (lo < hi) {
-          size_t mid = (lo + hi) / 2;
-          if (qb * qk[mid] >= tau)
-            lo = mid + 1;
-          else
-            hi = mid;
-        }
-        size_t nk = lo;
-        if (ca == cb) nk = std::min(nk, bp + 1);
-        size_t split = nk;
-        if (fp64_cut > 0.0) {
-          size_t l2 = 0, h2 = nk;
-          while (l2 < h2) {
-            size_t mid = (l2 + h2) / 2;
-            if (qb * qk[mid] >= fp64_cut)
-              l2 = mid + 1;
+        for (const auto& grp : groups) {
+          const size_t gs = grp.first, ge = grp.second;
+          if (ca == cb && gs > bp) break;  // kets at class positions <= bp only
+          size_t lo = gs, hi = ge;  // first ket with qb*qk < tau
+          while (lo < hi) {
+            size_t mid = (lo + hi) / 2;
+            if (qb * qk[mid] >= tau)
+              lo = mid + 1;
             else
-              h2 = mid;
+              hi = mid;
           }
-          split = l2;
+          size_t end = lo;
+          if (ca == cb) end = std::min(end, bp + 1);
+          if (end <= gs) continue;
+          size_t split = end;
+          if (fp64_cut > 0.0) {
+            size_t l2 = gs, h2 = end;
+            while (l2 < h2) {
+              size_t mid = (l2 + h2) / 2;
+              if (qb * qk[mid] >= fp64_cut)
+                l2 = mid + 1;
+              else
+                h2 = mid;
+            }
+            split = l2;
+          }
+          bras.push_back(B[bp]);
+          st64.push_back((int)gs);
+          n64.push_back((int)(split - gs));
+          st32.push_back((int)split);
+          n32.push_back((int)(end - split));
         }
-        bras[bp] = B[bp];
-        n64[bp] = (int)split;
-        n32[bp] = (int)(nk - split);
-        st32[bp] = (int)split;
       }
       const int* klist = P->d_class_lists.p + P->class_list_off[cb];
       int rc;
-      auto L64 = make_launch(P, ca, cb, false, bras, n64, {}, klist, 0, P->stream, rc);
+      auto L64 = make_launch(P, ca, cb, false, bras, n64, st64, klist, 0, P->stream, rc);
       if (!L64) return rc;
       ts.launches.push_back(std::move(L64));
       if (fp64_cut > 0.0) {
@@ -420,6 +548,7 @@ int igpu_plan_create(const igpu_shell* sh, size_t nsh, int engine, igpu_plan** o
     }
     d.atom = atom;
     if (d.spherical) P->spherical_any = true;
+    P->all_spherical = (s == 0 ? true : P->all_spherical) && d.spherical;
     P->shells.push_back(d);
   }
   P->nao = acc;
@@ -506,12 +635,23 @@ int igpu_plan_create(const igpu_shell* sh, size_t nsh, int engine, igpu_plan** o
   }
   rc = run_schwarz(P.get());
   if (rc) return rc;
-  // re-sort every class by Q descending (stable on pair index) for screening
+  // re-sort every class by (primitive-pair count desc, Q desc, index) and
+  // record the equal-count groups used to cut task segments
   {
     std::vector<int> flat;
+    P->class_groups.assign(npc, {});
     for (int c = 0; c < npc; ++c) {
       auto& v = P->class_pairs[c];
-      std::stable_sort(v.begin(), v.end(), [&](int x, int y) { return P->pairs[x].q > P->pairs[y].q; });
+      std::stable_sort(v.begin(), v.end(), [&](int x, int y) {
+        if (P->pairs[x].nprim != P->pairs[y].nprim) return P->pairs[x].nprim > P->pairs[y].nprim;
+        return P->pairs[x].q > P->pairs[y].q;
+      });
+      for (size_t a = 0; a < v.size();) {
+        size_t b = a;
+        while (b < v.size() && P->pairs[v[b]].nprim == P->pairs[v[a]].nprim) ++b;
+        P->class_groups[c].push_back({a, b});
+        a = b;
+      }
       P->class_list_off[c] = (int)flat.size();
       flat.insert(flat.end(), v.begin(), v.end());
     }
@@ -528,6 +668,7 @@ int igpu_plan_destroy(igpu_plan* plan) {
   cudaStreamSynchronize(plan->stream);
   if (plan->ev0) cudaEventDestroy(plan->ev0);
   if (plan->ev1) cudaEventDestroy(plan->ev1);
+  for (cudaEvent_t ev : plan->events) cudaEventDestroy(ev);
   cudaStream_t s = plan->stream;
   delete plan;
   if (s) cudaStreamDestroy(s);
@@ -637,31 +778,35 @@ int igpu_jk_device(igpu_plan* P, const double* d_dens, int ndens, const uint32_t
   A.mode = MODE_JK;
   A.jk.D = d_dens;
   A.jk.bounds = P->d_bounds.p;
-  A.jk.J = d_J;
-  A.jk.K = want_k ? d_K : nullptr;
   A.jk.ndens = ndens;
   A.jk.want_k = want_k ? 1 : 0;
   A.jk.symmetric = asym == 0 ? 1 : 0;
   A.jk.threshold = threshold;
   A.bra_bitmap = bra_subset ? P->d_bitmap.p : nullptr;
+  const size_t n2 = (size_t)P->nao * P->nao * ndens;
+  if (A.jk.symmetric) {
+    // one-orientation accumulators, symmetrised into the caller's J/K below
+    CK(P->d_Jh.ensure(n2));
+    CK(cudaMemsetAsync(P->d_Jh.p, 0, n2 * sizeof(double), s));
+    A.jk.J = P->d_Jh.p;
+    if (want_k) {
+      CK(P->d_Kh.ensure(n2));
+      CK(cudaMemsetAsync(P->d_Kh.p, 0, n2 * sizeof(double), s));
+      A.jk.K = P->d_Kh.p;
+    }
+  } else {
+    A.jk.J = d_J;
+    A.jk.K = want_k ? d_K : nullptr;
+  }
   uint32_t launches = 3;
-  CK(cudaEventRecord(P->ev0, s));
   int rc = run_tasks(P, *it->second, A, s, launches);
   if (rc) return rc;
-  CK(cudaEventRecord(P->ev1, s));
-  Counters c{};
-  CK(cudaMemcpyAsync(&c, P->d_counters.p, sizeof(c), cudaMemcpyDeviceToHost, s));
+  if (A.jk.symmetric) {
+    CK(launch_symmetrize_add(P->d_Jh.p, d_J, ndens, P->nao, s));
+    if (want_k) CK(launch_symmetrize_add(P->d_Kh.p, d_K, ndens, P->nao, s));
+  }
   CK(cudaStreamSynchronize(s));
-  float ms = 0.f;
-  cudaEventElapsedTime(&ms, P->ev0, P->ev1);
-  P->last = igpu_stats{};
-  P->last.quartets = c.quartets;
-  P->last.quartet_hash = c.hash;
-  P->last.quartets_fp32 = c.fp32_quartets;
-  P->last.prim_quartets = c.prim_quartets;
-  P->last.kernel_ms = ms;
-  P->last.launches = launches;
-  return IGPU_OK;
+  return collect_profile(P, ndens, true);
 }
 
 int igpu_jk(igpu_plan* P, const double* dens, int ndens, const uint32_t* bra_subset, size_t nsub, double threshold,
@@ -780,6 +925,13 @@ int igpu_eri_builder_fill(igpu_plan* P, const uint32_t* sub, size_t nsub, double
 int igpu_last_stats(const igpu_plan* P, igpu_stats* st) {
   if (!P || !st) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
   *st = P->last;
+  return IGPU_OK;
+}
+
+int igpu_last_profile(const igpu_plan* P, igpu_launch_record* out, size_t cap, size_t* n) {
+  if (!P || !n) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  *n = P->profile.size();
+  for (size_t k = 0; k < P->profile.size() && k < cap && out; ++k) out[k] = P->profile[k];
   return IGPU_OK;
 }
 

@@ -317,27 +317,90 @@ __device__ __forceinline__ void jk_term(const double* B, const int dims[4], cons
   }
 }
 
+// Bra-block J term accumulated across consecutive quartets of one bra pair
+// (the J' entries of the evaluation bra block change only when the bra does):
+// acc[q] += w * sum_{cd} B[ab cd] D[C c][D d], flushed by flush_bra_acc.
+__device__ __forceinline__ void jk_term_acc(const double* B, const int dims[4], const int offs[4], int nao,
+                                            const double* Dm, double w, double* acc, int lane, int T) {
+  const int st1 = dims[2] * dims[3];
+  const int nu = dims[0], nv = dims[1], ns = dims[2], nt = dims[3];
+  for (int q = lane; q < nu * nv; q += T) {
+    const double* row = B + (size_t)q * st1;
+    double s = 0.0;
+    for (int is = 0; is < ns; ++is) {
+      const double* drow = Dm + (size_t)(offs[2] + is) * nao + offs[3];
+      for (int it = 0; it < nt; ++it) s += row[is * nt + it] * __ldg(drow + it);
+    }
+    acc[q] += w * s;
+  }
+}
+
+// Atomically add a team's running bra-block accumulators to J' and clear
+// them.  acc layout: [0] = evaluation bra pair index (or -1), then
+// ndens blocks of n_func(A) x n_func(B).
+__device__ __forceinline__ void flush_bra_acc(const KernelArgs& A, double* acc, int lane, int T, unsigned tmask) {
+  const int bra = (int)acc[0];
+  if (bra >= 0) {
+    const PairD pb = A.pairs[bra];
+    const DevShell sa = A.shells[pb.a], sb = A.shells[pb.b];
+    const int nab = sa.nfunc * sb.nfunc;
+    const size_t n2 = (size_t)A.nao * A.nao;
+    for (int d = 0; d < A.jk.ndens; ++d) {
+      double* a = acc + 1 + (size_t)d * nab;
+      for (int q = lane; q < nab; q += T) {
+        const double v = a[q];
+        if (v != 0.0) {
+          const int ia = q / sb.nfunc, ib = q % sb.nfunc;
+          atomicAdd(A.jk.J + d * n2 + (size_t)(sa.off + ia) * A.nao + sb.off + ib, v);
+          a[q] = 0.0;
+        }
+      }
+    }
+  }
+  __syncwarp(tmask);
+  if (lane == 0) acc[0] = -1.0;
+  __syncwarp(tmask);
+}
+
 __device__ __forceinline__ void consume_jk(const KernelArgs& A, const double* B, const int dims[4],
-                                           const int offs[4], const int sh[4], uint64_t mask, int lane, int T) {
+                                           const int offs[4], const int sh[4], uint64_t mask, int lane, int T,
+                                           double* acc, int pbi, unsigned tmask) {
   const unsigned w = distinct_perms(sh);
   auto W = [&](int p) { return (double)((w >> p) & 1u); };
   const int nao = A.nao;
   const size_t n2 = (size_t)nao * nao;
+  if (A.jk.symmetric) {
+    // One orientation of every image: J'[A a][B b], J'[C c][D d], K'[A a][C c],
+    // K'[B b][C c], K'[A a][D d], K'[B b][D d] with the summed weights of the
+    // permutations landing on the block or its transpose.
+    if ((int)acc[0] != pbi) {
+      flush_bra_acc(A, acc, lane, T, tmask);
+      if (lane == 0) acc[0] = (double)pbi;
+      __syncwarp(tmask);
+    }
+    const int nab = dims[0] * dims[1];
+    for (int d = 0; d < A.jk.ndens; ++d) {
+      if (!((mask >> d) & 1ull)) continue;
+      const double* Dm = A.jk.D + d * n2;
+      double* J = A.jk.J + d * n2;
+      double* K = A.jk.want_k ? A.jk.K + d * n2 : nullptr;
+      jk_term_acc(B, dims, offs, nao, Dm, W(0) + W(1) + W(2) + W(3), acc + 1 + (size_t)d * nab, lane, T);
+      jk_term(B, dims, offs, nao, 2, 3, 0, 1, Dm, 0, 1, J, W(4) + W(5) + W(6) + W(7), J, 0.0, lane, T);
+      if (K) {
+        jk_term(B, dims, offs, nao, 0, 2, 1, 3, Dm, 1, 3, K, W(0) + W(4), K, 0.0, lane, T);
+        jk_term(B, dims, offs, nao, 1, 2, 0, 3, Dm, 0, 3, K, W(1) + W(5), K, 0.0, lane, T);
+        jk_term(B, dims, offs, nao, 0, 3, 1, 2, Dm, 1, 2, K, W(2) + W(6), K, 0.0, lane, T);
+        jk_term(B, dims, offs, nao, 1, 3, 0, 2, Dm, 0, 2, K, W(3) + W(7), K, 0.0, lane, T);
+      }
+    }
+    return;
+  }
   for (int d = 0; d < A.jk.ndens; ++d) {
     if (!((mask >> d) & 1ull)) continue;
     const double* Dm = A.jk.D + d * n2;
     double* J = A.jk.J + d * n2;
     double* K = A.jk.want_k ? A.jk.K + d * n2 : nullptr;
-    if (A.jk.symmetric) {
-      jk_term(B, dims, offs, nao, 0, 1, 2, 3, Dm, 2, 3, J, W(0) + W(2), J, W(1) + W(3), lane, T);
-      jk_term(B, dims, offs, nao, 2, 3, 0, 1, Dm, 0, 1, J, W(4) + W(5), J, W(6) + W(7), lane, T);
-      if (K) {
-        jk_term(B, dims, offs, nao, 0, 2, 1, 3, Dm, 1, 3, K, W(0), K, W(4), lane, T);
-        jk_term(B, dims, offs, nao, 1, 2, 0, 3, Dm, 0, 3, K, W(1), K, W(5), lane, T);
-        jk_term(B, dims, offs, nao, 0, 3, 1, 2, Dm, 1, 2, K, W(2), K, W(6), lane, T);
-        jk_term(B, dims, offs, nao, 1, 3, 0, 2, Dm, 0, 2, K, W(3), K, W(7), lane, T);
-      }
-    } else {
+    {
       // P0..P3 J on (A,B); P4..P7 J on (C,D)
       jk_term(B, dims, offs, nao, 0, 1, 2, 3, Dm, 2, 3, J, W(0), J, W(1), lane, T);
       jk_term(B, dims, offs, nao, 0, 1, 2, 3, Dm, 3, 2, J, W(2), J, W(3), lane, T);
@@ -454,7 +517,7 @@ __device__ __forceinline__ void post_quartet(const KernelArgs& A, const ClassDim
   const int offs[4] = {s0.off, s1.off, s2.off, s3.off};
   switch (A.mode) {
     case MODE_JK:
-      consume_jk(A, B, dims, offs, shl, sc.mask, lane, T);
+      consume_jk(A, B, dims, offs, shl, sc.mask, lane, T, slot + A.acc_offset, pb_index, tmask);
       break;
     case MODE_DENSE:
       consume_dense(A, B, dims, offs, shl, lane, T);

@@ -12,15 +12,17 @@
 // early-contraction scheme of the reference's OS/HGP engine
 // (src/engine/os_eri.rs:1-12) applied to Rys 2D integrals.
 //   TEAM == 1 : one thread per quartet, everything in registers.
-//   TEAM >= 8 : a team of TEAM lanes per quartet; roots and the 3*nroots
+//   TEAM >= 2 : a team of TEAM lanes per quartet; roots and the 3*nroots
 //               per-axis tables are built cooperatively in shared memory and
 //               every lane accumulates its own rows e of G (register tiles
 //               of FCH columns, the f range walked in chunks).
+// The class's Rys Chebyshev table is staged in shared memory per block.
 // Phase 2 (post.cuh) runs the horizontal recurrences, the Cartesian ->
 // spherical transform and the mode-specific consumer on the team.
 #pragma once
 #include "device_common.cuh"
 #include "post.cuh"
+#include "post_thread.cuh"
 
 namespace igpu {
 
@@ -35,15 +37,19 @@ struct ClassShape {
   static constexpr int NG = NEP * NFP;
 };
 
-// Team size per class: one thread while the whole G table fits comfortably
-// in registers, otherwise the smallest power-of-two team covering the rows.
-template <int LA, int LB, int LC, int LD>
-__host__ __device__ constexpr int team_size() {
-  constexpr int nep = nrange(LA, LA + LB), nfp = nrange(LC, LC + LD);
+// Lanes per quartet: one thread while the whole G table fits in registers,
+// otherwise the smallest team of 8, 16 or 32 lanes covering the rows (teams
+// of 2 or 4 lanes measured slower: the per-primitive root and recurrence
+// work is then spread over too few lanes).
+__host__ __device__ constexpr int team_for(int nep, int nfp) {
   if (nep * nfp <= 81) return 1;
   if (nep <= 8) return 8;
   if (nep <= 16) return 16;
   return 32;
+}
+template <int LA, int LB, int LC, int LD>
+__host__ __device__ constexpr int team_size() {
+  return team_for(nrange(LA, LA + LB), nrange(LC, LC + LD));
 }
 
 // Phase-1 register footprint per lane: rows x FCH accumulators.
@@ -67,8 +73,8 @@ struct TeamShape {
 // ------------------------------------------------------------- TEAM == 1
 
 template <int LA, int LB, int LC, int LD, typename R>
-__device__ __forceinline__ void accumulate_thread(const KernelArgs& A, const PairD& pb, const PairD& pk,
-                                                  R (&G)[ClassShape<LA, LB, LC, LD>::NG]) {
+__device__ __forceinline__ void accumulate_thread(const KernelArgs& A, const R* s_tab, const PairD& pb,
+                                                  const PairD& pk, R (&G)[ClassShape<LA, LB, LC, LD>::NG]) {
   using S = ClassShape<LA, LB, LC, LD>;
   constexpr int NE = S::NE, NF = S::NF, NR = S::NR;
 #pragma unroll
@@ -79,7 +85,7 @@ __device__ __forceinline__ void accumulate_thread(const KernelArgs& A, const Pai
       const PrimPairD kp = A.prims[pk.prim_off + kq];
       const QuartetHdr<R> h = quartet_header<R>(bp, kp);
       R x[NR], w[NR];
-      rys_roots<NR, R>(h.T, x, w);
+      rys_roots_s<NR, R>(s_tab, h.T, x, w);
       const R inv_pq = R(1) / h.pq;
       const R qpq = h.q * inv_pq, ppq = h.p * inv_pq;
       const R inv2pq = R(0.5) * inv_pq, inv2p = R(0.5) / h.p, inv2q = R(0.5) / h.q;
@@ -112,9 +118,9 @@ __device__ __forceinline__ void accumulate_thread(const KernelArgs& A, const Pai
 
 // --------------------------------------------------------------- TEAM > 1
 
-// Root r of the N-point quadrature (one lane per root).
+// Root r of the N-point quadrature from the shared-memory table.
 template <int N, typename R>
-__device__ __forceinline__ void rys_root_one(R T, int r, R& x, R& w) {
+__device__ __forceinline__ void rys_root_one(const R* s_tab, R T, int r, R& x, R& w) {
   const RysMeta m = c_rys[N];
   if (T >= R(m.t_hi)) {
     if constexpr (sizeof(R) == 8) {
@@ -132,20 +138,16 @@ __device__ __forceinline__ void rys_root_one(R T, int r, R& x, R& w) {
   R a = R(s) * width;
   R b = a + width;
   R xi = (R(2) * T - (a + b)) / (b - a);
-  const R* base;
-  if constexpr (sizeof(R) == 8)
-    base = c_rys_tab + m.off + ((size_t)s * N + r) * 2 * RYS_NC;
-  else
-    base = c_rys_tab_f + m.off + ((size_t)s * N + r) * 2 * RYS_NC;
-  x = chebev<R>(base, xi);
-  w = chebev<R>(base + RYS_NC, xi);
+  const R* base = s_tab + ((size_t)s * N + r) * 2 * RYS_NC;
+  x = chebev_s<R>(base, xi);
+  w = chebev_s<R>(base + RYS_NC, xi);
 }
 
 // One pass over all primitive quartets accumulating the columns
 // [F0, F0 + FCH) of this lane's rows.
 template <int LA, int LB, int LC, int LD, typename R, int F0>
-__device__ __forceinline__ void team_pass(const KernelArgs& A, const PairD& pb, const PairD& pk, R* sm,
-                                          int lane, unsigned tmask, double* G) {
+__device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, const PairD& pb, const PairD& pk,
+                                          R* sm, int lane, unsigned tmask, double* G) {
   using S = ClassShape<LA, LB, LC, LD>;
   using TS = TeamShape<LA, LB, LC, LD, R>;
   constexpr int NE = S::NE, NF = S::NF, NR = S::NR, T = TS::T;
@@ -175,18 +177,18 @@ __device__ __forceinline__ void team_pass(const KernelArgs& A, const PairD& pb, 
       R* xs = B;
       R* ws = B + NR;
       R* gt = B + 2 * NR;
-      if (lane < NR) {
+      for (int r = lane; r < NR; r += T) {
         R xr, wr;
-        rys_root_one<NR, R>(h.T, lane, xr, wr);
-        xs[lane] = xr;
-        ws[lane] = wr * h.pref;
+        rys_root_one<NR, R>(s_tab, h.T, r, xr, wr);
+        xs[r] = xr;
+        ws[r] = wr * h.pref;
       }
       __syncwarp(tmask);
-      if (lane < 3 * NR) {
-        const int axis = lane / NR, r = lane - axis * NR;
-        const R inv_pq = R(1) / h.pq;
+      const R inv_pq = R(1) / h.pq;
+      const R qpq = h.q * inv_pq, ppq = h.p * inv_pq;
+      for (int t = lane; t < 3 * NR; t += T) {
+        const int axis = t / NR, r = t - axis * NR;
         const R xr = xs[r];
-        const R qpq = h.q * inv_pq, ppq = h.p * inv_pq;
         const R b00 = xr * R(0.5) * inv_pq;
         const R b10 = (R(1) - xr * qpq) * (R(0.5) / h.p);
         const R b01 = (R(1) - xr * ppq) * (R(0.5) / h.q);
@@ -239,13 +241,13 @@ __device__ __forceinline__ void team_pass(const KernelArgs& A, const PairD& pb, 
 }
 
 template <int LA, int LB, int LC, int LD, typename R, int C>
-__device__ __forceinline__ void team_chunks(const KernelArgs& A, const PairD& pb, const PairD& pk, R* sm,
-                                            int lane, unsigned tmask, double* G) {
+__device__ __forceinline__ void team_chunks(const KernelArgs& A, const R* s_tab, const PairD& pb, const PairD& pk,
+                                            R* sm, int lane, unsigned tmask, double* G) {
   using TS = TeamShape<LA, LB, LC, LD, R>;
   if constexpr (C < TS::NCHUNK) {
-    team_pass<LA, LB, LC, LD, R, C * TS::FCH>(A, pb, pk, sm, lane, tmask, G);
+    team_pass<LA, LB, LC, LD, R, C * TS::FCH>(A, s_tab, pb, pk, sm, lane, tmask, G);
     __syncwarp(tmask);
-    team_chunks<LA, LB, LC, LD, R, C + 1>(A, pb, pk, sm, lane, tmask, G);
+    team_chunks<LA, LB, LC, LD, R, C + 1>(A, s_tab, pb, pk, sm, lane, tmask, G);
   }
 }
 
@@ -257,6 +259,8 @@ __global__ void __launch_bounds__(128) quartet_kernel(KernelArgs A) {
   using TS = TeamShape<LA, LB, LC, LD, R>;
   constexpr int T = TS::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ R s_tab[S::NR * RYS_MAX_SUB * 2 * RYS_NC];
+  stage_rys_table<S::NR, R>(s_tab);
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int team = tid / T;
   const int lane = threadIdx.x % T;
@@ -266,27 +270,61 @@ __global__ void __launch_bounds__(128) quartet_kernel(KernelArgs A) {
   double* slot = A.scratch + (size_t)team * A.slot_doubles;
   QuartetCounters cnt;
   const ClassDims dims{LA, LB, LC, LD};
-
-  for (unsigned long long g = team; g < A.task.total; g += nteams) {
-    int pbi, pki;
-    decode_task(A.task, g, pbi, pki);
-    const PairD pb = A.pairs[pbi];
-    const PairD pk = A.pairs[pki];
-    Screen sc = screen_quartet(A, pb, pk);
-    if (!sc.keep) continue;
-    if (lane == 0) cnt.add(sc, pb, pk, A.fp32);
-    if constexpr (T == 1) {
-      R G[S::NG];
-      accumulate_thread<LA, LB, LC, LD, R>(A, pb, pk, G);
-#pragma unroll
-      for (int q = 0; q < S::NG; ++q) slot[q] = (double)G[q];
-    } else {
-      team_chunks<LA, LB, LC, LD, R, 0>(A, pb, pk, sm, lane, tmask, slot);
-    }
-    __syncwarp(tmask);
-    post_quartet(A, dims, pb, pk, sc, slot, lane, T, tmask, pbi);
-    __syncwarp(tmask);
+  (void)nteams;
+  const bool use_acc = A.mode == MODE_JK && A.jk.symmetric;
+  if (use_acc) {
+    // the scratch slot is shared with earlier launches: clear the running
+    // bra-block accumulators before first use
+    double* acc = slot + A.acc_offset;
+    const int nacc = A.jk.ndens * ncart(LA) * ncart(LB);
+    for (int q = lane; q < nacc; q += T) acc[1 + q] = 0.0;
+    if (lane == 0) acc[0] = -1.0;
   }
+  __syncwarp(tmask);
+
+  // Warps claim contiguous chunks of the task list; the teams of a warp
+  // interleave inside a chunk, so consecutive quartets (same bra pair, same
+  // primitive-pair count) stay on the same lanes.
+  constexpr int TPW = 32 / T;
+  const int tw = (threadIdx.x & 31) / T;
+  for (;;) {
+    unsigned long long base = 0;
+    if ((threadIdx.x & 31) == 0) base = atomicAdd(A.work_counter, A.chunk);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= A.task.total) break;
+    const unsigned long long end = base + A.chunk < A.task.total ? base + A.chunk : A.task.total;
+    for (unsigned long long g = base + tw; g < end; g += TPW) {
+      int pbi, pki;
+      decode_task(A.task, g, pbi, pki);
+      const PairD pb = A.pairs[pbi];
+      const PairD pk = A.pairs[pki];
+      Screen sc = screen_quartet(A, pb, pk);
+      if (!sc.keep) continue;
+      if (lane == 0) cnt.add(sc, pb, pk, A.fp32);
+      if constexpr (T == 1) {
+        R G[S::NG];
+        accumulate_thread<LA, LB, LC, LD, R>(A, s_tab, pb, pk, G);
+        if (use_acc && A.kinds != 2) {
+          double Gd[S::NG];
+#pragma unroll
+          for (int q = 0; q < S::NG; ++q) Gd[q] = (double)G[q];
+          if (A.kinds == 0)
+            thread_post_jk<LA, LB, LC, LD, false>(A, Gd, pb, pk, sc, slot + A.acc_offset, pbi);
+          else
+            thread_post_jk<LA, LB, LC, LD, true>(A, Gd, pb, pk, sc, slot + A.acc_offset, pbi);
+          continue;
+        }
+#pragma unroll
+        for (int q = 0; q < S::NG; ++q) slot[q] = (double)G[q];
+      } else {
+        team_chunks<LA, LB, LC, LD, R, 0>(A, s_tab, pb, pk, sm, lane, tmask, slot);
+      }
+      __syncwarp(tmask);
+      post_quartet(A, dims, pb, pk, sc, slot, lane, T, tmask, pbi);
+      __syncwarp(tmask);
+    }
+  }
+  if (use_acc) flush_bra_acc(A, slot + A.acc_offset, lane, T, tmask);
   cnt.flush(A.counters);
 }
 
