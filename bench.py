@@ -1,0 +1,394 @@
+"""Benchmark: integral-direct Fock J/K build on B200.
+
+Workload (the reference's headline J/K configuration): 64 atoms placed at
+random in a 20-bohr cube (min separation 1.8 bohr), Cartesian shells
+s,s,s,p,p,d of 3 primitives with even-tempered exponents 0.1*2.5^k and
+contraction coefficients U(0.2,1.0) -> nao = 960; four symmetric densities
+D = C C^T with C (960 x 80) ~ N(0, 1/sqrt(nao)); Schwarz threshold 1e-12.
+Synthetic, seeded (no data set exists for this benchmark).
+
+A step is one full J+K build over every canonical bra pair.  `value` is
+screened canonical shell quartets per second in the FP32-mixed mode (the
+FP64 path is reported beside it, with the mixed-vs-FP64 energy error),
+device-timed with CUDA events on the launching stream, inputs resident in
+HBM, L2 flushed between steps.  `e2e` is the same metric through the C ABI
+with host buffers (pinned), including the H2D of the densities and the D2H
+of J and K.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun), every rank builds J/K for an interleaved share of the
+canonical bra pairs and one NCCL all-reduce sums the partial J and K: the
+total work is fixed (strong scaling); time = max over ranks.
+
+`--impl reference` times the reference algorithm on the host cores: the C++
+restatement of the reference's CPU path (the Rust crate cannot be built in
+this image), all threads, each step a seeded sample of bra pairs.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Fock J/K build quartets/s (FP32-mixed, <=1e-6 Eh vs FP64) on B200"
+UNIT = "quartets/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--cpu-sample-bras", type=int, default=24)
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.idx)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------- peaks
+
+def measured_gemm_tflops(torch, dtype, n=8192, reps=5):
+    """Library GEMM rate on this GPU (cuBLAS), the compute-peak reference of
+    the roofline: float64 (FP64 pipe) and float32 without TF32."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(n, n, device="cuda", dtype=dtype)
+    b = torch.randn(n, n, device="cuda", dtype=dtype)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+# --------------------------------------------------------------- CPU side
+
+def cpu_plan(system):
+    """The restated reference plan (Schwarz bounds built here, outside any
+    timing)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_py as O
+    B = O.OracleBasis(system["shells"])
+    B.direct_schwarz()
+    return B
+
+
+def cpu_rate(B, system, nbras, seed, nthreads):
+    """Screened quartets/s of the C++ restatement of the reference CPU path
+    (bra pair as the grain, one workspace and private J/K per worker) over a
+    seeded sample of canonical bra pairs."""
+    nsh = len(system["shells"])
+    nbra = nsh * (nsh + 1) // 2
+    bras = np.random.default_rng(seed).choice(nbra, nbras, replace=False)
+    t0 = time.perf_counter()
+    _, _, cnt, _ = B.direct_jk(system["dens"], system["threshold"], bras=bras, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return cnt / dt, cnt, dt, nbras
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from integral_b200 import systems as S
+    system = S.jk_system()
+    nthreads = os.cpu_count() or 1
+    rates = []
+    B = cpu_plan(system)
+    for step in range(args.warmup + args.steps):
+        r, cnt, dt, nb = cpu_rate(B, system, max(4, args.cpu_sample_bras // 3), 1000 + step, nthreads)
+        if step >= args.warmup:
+            rates.append(r)
+    val = float(statistics.mean(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": "direct J/K, 64 atoms, nao 960, 4 densities, tau 1e-12", "nao": 960,
+                   "ndens": 4, "threshold": 1e-12},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": nthreads, "kind": "port",
+                         "sample": "%d seeded canonical bra pairs per step (of 73920), all threads; C++ "
+                                   "restatement of the reference CPU path (Rust toolchain absent)"
+                                   % max(4, args.cpu_sample_bras // 3)},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# --------------------------------------------------------------- GPU side
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import integral_b200 as ib
+    from integral_b200 import sharding
+    from integral_b200 import systems as S
+
+    system = S.jk_system()
+    nao = S.nao_of(system["shells"])
+    nd = system["dens"].shape[0]
+    thr = system["threshold"]
+    basis = ib.Basis(system["shells"])
+    dc = basis.direct_contractor()
+    nbra = len(dc.bra_pairs())
+    bras = None if world == 1 else sharding.bra_shard(nbra, rank, world)
+
+    D = torch.from_numpy(system["dens"]).cuda()
+    J = torch.zeros_like(D)
+    K = torch.zeros_like(D)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float64, device="cuda")  # 512 MB > L2
+    stream = torch.cuda.current_stream()
+
+    def step(prec):
+        J.zero_()
+        K.zero_()
+        dc.jk_device(D.data_ptr(), nd, J.data_ptr(), K.data_ptr(), thr, True, prec, bras=bras,
+                     stream=stream.cuda_stream)
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(J)
+            dist.all_reduce(K)
+
+    def timed(prec, warm, steps, sampler=None):
+        for _ in range(warm):
+            step(prec)
+        torch.cuda.synchronize()
+        times, quartets, launches = [], 0, 0
+        prof = None
+        if sampler:
+            sampler.start()
+        for _ in range(steps):
+            flush.fill_(1.0)
+            if world > 1:
+                import torch.distributed as dist
+                dist.barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step(prec)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            st = dc.last_stats()
+            quartets += st["quartets"]
+            launches += st["launches"] + 4  # + bounds, symmetry check, 2 symmetrisations
+            prof = dc.plan.profile()
+        clocks = sampler.stop() if sampler else None
+        t = sum(times)
+        if world > 1:
+            import torch.distributed as dist
+            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+            qq = torch.tensor([float(quartets)], device="cuda", dtype=torch.float64)
+            dist.all_reduce(qq)
+            quartets = int(qq.item())
+        return t, quartets, launches, prof, clocks
+
+    sampler = ClockSampler(local) if rank == 0 else None
+    t_mixed, q_mixed, l_mixed, prof_mixed, clocks = timed(1, args.warmup, args.steps, sampler)
+    Jm, Km = J.cpu().numpy().copy(), K.cpu().numpy().copy()
+    t_64, q_64, l_64, prof_64, _ = timed(0, 1, args.steps)
+    J64, K64 = J.cpu().numpy(), K.cpu().numpy()
+    Dn = system["dens"]
+
+    def energy(Jx, Kx):
+        return sum(0.5 * float(np.sum(Dn[d] * (Jx[d] - 0.5 * Kx[d]))) for d in range(nd))
+
+    dE = energy(Jm, Km) - energy(J64, K64)
+
+    # end to end through the C ABI with pinned host buffers
+    Dh = torch.from_numpy(system["dens"]).pin_memory()
+    Jh = torch.zeros(Dh.shape, dtype=torch.float64).pin_memory()
+    Kh = torch.zeros(Dh.shape, dtype=torch.float64).pin_memory()
+    from integral_b200 import _lib
+    L = _lib.lib()
+    sub = None if bras is None else np.ascontiguousarray(bras, dtype=np.uint32)
+
+    def e2e_step():
+        Jh.zero_()
+        Kh.zero_()
+        _lib.check(L.igpu_jk(dc.plan.h, _lib.ctypes.cast(_lib.ctypes.c_void_p(Dh.data_ptr()), _lib.c_double_p), nd,
+                             sub.ctypes.data_as(_lib.c_u32_p) if sub is not None else None,
+                             0 if sub is None else len(sub), thr, 1, 1,
+                             _lib.ctypes.cast(_lib.ctypes.c_void_p(Jh.data_ptr()), _lib.c_double_p),
+                             _lib.ctypes.cast(_lib.ctypes.c_void_p(Kh.data_ptr()), _lib.c_double_p)))
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(Jh)
+            dist.all_reduce(Kh)
+
+    e2e_step()
+    te = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        torch.cuda.synchronize()
+        te += time.perf_counter() - t0
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([te], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+
+    fp64_peak = measured_gemm_tflops(torch, torch.float64)
+    fp32_peak = measured_gemm_tflops(torch, torch.float32)
+    top = max(prof_mixed, key=lambda r: r["ms"])
+    achieved = top["model_flops"] / (top["ms"] * 1e-3) / 1e12
+    pk = fp32_peak if top["fp32"] else fp64_peak
+    total_model = sum(r["model_flops"] for r in prof_mixed)
+    kernel_ms = sum(r["ms"] for r in prof_mixed)
+
+    cpu = None
+    if world == 1:
+        r, cnt, dt, nb = cpu_rate(cpu_plan(system), system, args.cpu_sample_bras, 7, os.cpu_count() or 1)
+        cpu = {"value": r, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": "%d seeded canonical bra pairs of 73920 (%d screened quartets, %.1f s), all threads; "
+                         "C++ restatement of the reference CPU path" % (nb, cnt, dt)}
+
+    steps = args.steps
+    line = {
+        "metric": METRIC,
+        "value": q_mixed / (t_mixed * 1e-3),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_mixed / steps,
+        "higher_is_better": True,
+        "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "fp32-mixed (fp64 accumulation)",
+        "data": "synthetic (seeded generator, no data set)",
+        "config": {"workload": "direct J/K, 64 atoms in 20-bohr cube, s,s,s,p,p,d Cartesian, nao 960, "
+                               "4 densities, Schwarz tau 1e-12",
+                   "nao": nao, "ndens": nd, "threshold": thr, "quartets_per_step": q_mixed // steps,
+                   "parallelism": "bra-pair shards x%d + NCCL all-reduce" % world if world > 1 else "1 GPU",
+                   "l2": "flushed between steps (512 MB write)"},
+        "fp64": {"value": q_64 / (t_64 * 1e-3), "unit": UNIT, "ms_per_step": t_64 / steps,
+                 "mixed_speedup": (t_64 / t_mixed), "energy_error_mixed_vs_fp64_Eh": dE},
+        "e2e": {"value": q_mixed / te if te > 0 else None, "unit": UNIT,
+                "h2d_bytes_per_step": int(Dh.numel() * 8), "d2h_bytes_per_step": int(2 * Jh.numel() * 8)},
+        "roofline": {"bound": "fp32" if top["fp32"] else "fp64",
+                     "kernel": "quartet_kernel(%d%d|%d%d) %s" % (top["la"], top["lb"], top["lc"], top["ld"],
+                                                                 "fp32" if top["fp32"] else "fp64"),
+                     "achieved": achieved, "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk,
+                     "peak_source": "cuBLAS %s GEMM measured in this run (no FP64/FP32 CUDA-core peak in "
+                                    "MEASURED_PEAKS.json)" % ("SGEMM, TF32 off" if top["fp32"] else "DGEMM"),
+                     "flops_model": "fixed Rys flop model of the reference algorithm per surviving primitive "
+                                    "quartet (+J/K contraction)",
+                     "traffic": None,
+                     "all_kernels_model_tflops": total_model / (kernel_ms * 1e-3) / 1e12},
+        "clocks": clocks,
+        "gpu_launches": l_mixed,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

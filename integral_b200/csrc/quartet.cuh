@@ -64,10 +64,15 @@ struct TeamShape {
   static constexpr int FCH0 = max_acc<R>() / ROWS;
   static constexpr int FCH = FCH0 < 1 ? 1 : (FCH0 > S::NFP ? S::NFP : FCH0);
   static constexpr int NCHUNK = (S::NFP + FCH - 1) / FCH;
-  // shared memory per team and buffer: x[NR], w[NR], g[3][NR][NE+1][NF+1]
+  // Primitive quartets set up per round: as many as fit a shared-memory
+  // budget of 48 KB per 128-thread block (power of two, at most T).
   static constexpr int GTAB = (S::NE + 1) * (S::NF + 1);
-  static constexpr int BUF = 2 * S::NR + 3 * S::NR * GTAB;
-  static constexpr int SMEM_PER_TEAM = T == 1 ? 0 : 2 * BUF;  // in R units
+  static constexpr int PRIM_TAB = 2 * S::NR + 3 * S::NR * GTAB;  // x, w, g[3][NR][GTAB]
+  static constexpr int BUDGET = (48 * 1024 / 128) * (T == 1 ? 1 : T) / (int)sizeof(R);
+  static constexpr int BP0 = BUDGET / PRIM_TAB;
+  static constexpr int BP = BP0 >= T ? T : (BP0 >= 16 ? 16 : (BP0 >= 8 ? 8 : (BP0 >= 4 ? 4 : (BP0 >= 2 ? 2 : 1))));
+  static constexpr int SUB = T / BP;  // lanes sharing one primitive quartet in a round
+  static constexpr int SMEM_PER_TEAM = T == 1 ? 0 : BP * PRIM_TAB;  // in R units
 };
 
 // ------------------------------------------------------------- TEAM == 1
@@ -167,44 +172,57 @@ __device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, c
     ey[k] = addr_ly(a);
     ez[k] = addr_lz(a);
   }
-  int buf = 0;
-  for (int ip = 0; ip < pb.nprim; ++ip) {
-    const PrimPairD bp = A.prims[pb.prim_off + ip];
-    for (int kq = 0; kq < pk.nprim; ++kq) {
-      const PrimPairD kp = A.prims[pk.prim_off + kq];
-      const QuartetHdr<R> h = quartet_header<R>(bp, kp);
-      R* B = sm + buf * TS::BUF;
-      R* xs = B;
-      R* ws = B + NR;
-      R* gt = B + 2 * NR;
-      for (int r = lane; r < NR; r += T) {
+  // Rounds of BP primitive quartets: SUB lanes set up each one (roots, then
+  // the 3*NR per-axis tables) into its shared-memory slot, then every lane
+  // accumulates its rows over the whole round.
+  constexpr int BP = TS::BP, SUB = TS::SUB, PT = TS::PRIM_TAB;
+  const int npk = pk.nprim;
+  const int npr = pb.nprim * npk;
+  const int myp = lane % BP;
+  const int sub = lane / BP;
+  for (int base = 0; base < npr; base += BP) {
+    const int nb = npr - base < BP ? npr - base : BP;
+    const bool active = myp < nb;
+    R* mys = sm + myp * PT;
+    QuartetHdr<R> h;
+    if (active) {
+      const int pidx = base + myp;
+      const int ip = pidx / npk, kq = pidx - ip * npk;
+      h = quartet_header<R>(A.prims[pb.prim_off + ip], A.prims[pk.prim_off + kq]);
+      for (int r = sub; r < NR; r += SUB) {
         R xr, wr;
         rys_root_one<NR, R>(s_tab, h.T, r, xr, wr);
-        xs[r] = xr;
-        ws[r] = wr * h.pref;
+        mys[r] = xr;
+        mys[NR + r] = wr * h.pref;
       }
-      __syncwarp(tmask);
+    }
+    __syncwarp(tmask);
+    if (active) {
       const R inv_pq = R(1) / h.pq;
       const R qpq = h.q * inv_pq, ppq = h.p * inv_pq;
-      for (int t = lane; t < 3 * NR; t += T) {
+      const R inv2p = R(0.5) / h.p, inv2q = R(0.5) / h.q;
+      for (int t = sub; t < 3 * NR; t += SUB) {
         const int axis = t / NR, r = t - axis * NR;
-        const R xr = xs[r];
+        const R xr = mys[r];
         const R b00 = xr * R(0.5) * inv_pq;
-        const R b10 = (R(1) - xr * qpq) * (R(0.5) / h.p);
-        const R b01 = (R(1) - xr * ppq) * (R(0.5) / h.q);
+        const R b10 = (R(1) - xr * qpq) * inv2p;
+        const R b01 = (R(1) - xr * ppq) * inv2q;
         const R pqa = axis == 0 ? h.pqx : (axis == 1 ? h.pqy : h.pqz);
         const R paa = axis == 0 ? h.pax : (axis == 1 ? h.pay : h.paz);
         const R qca = axis == 0 ? h.qcx : (axis == 1 ? h.qcy : h.qcz);
         R g[NE + 1][NF + 1];
-        vrr_axis<NE, NF, R>(axis == 2 ? ws[r] : R(1), paa - xr * qpq * pqa, qca + xr * ppq * pqa, b10, b01,
+        vrr_axis<NE, NF, R>(axis == 2 ? mys[NR + r] : R(1), paa - xr * qpq * pqa, qca + xr * ppq * pqa, b10, b01,
                             b00, g);
-        R* dst = gt + (axis * NR + r) * GT;
+        R* dst = mys + 2 * NR + (axis * NR + r) * GT;
 #pragma unroll
         for (int n = 0; n <= NE; ++n)
 #pragma unroll
           for (int m = 0; m <= NF; ++m) dst[n * (NF + 1) + m] = g[n][m];
       }
-      __syncwarp(tmask);
+    }
+    __syncwarp(tmask);
+    for (int p = 0; p < nb; ++p) {
+      const R* gt = sm + p * PT + 2 * NR;
 #pragma unroll
       for (int r = 0; r < NR; ++r) {
         const R* tx = gt + (0 * NR + r) * GT;
@@ -227,8 +245,8 @@ __device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, c
           });
         }
       }
-      buf ^= 1;
     }
+    __syncwarp(tmask);
   }
 #pragma unroll
   for (int k = 0; k < TS::ROWS; ++k) {

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <stdexcept>
+#include <thread>
 
 #include "oracle.hpp"
 
@@ -197,10 +198,12 @@ std::vector<double> Basis::eri(Engine e) const {
 }
 
 // integrals.rs:842-862
+// Every entry is an independent evaluation, so rows are spread over host
+// threads (each entry's arithmetic is unchanged).
 std::vector<double> Basis::schwarz(Engine e) const {
   int n = nsh();
   std::vector<double> q((size_t)n * n, 0.0);
-  for (int i = 0; i < n; ++i)
+  auto row = [&](int i) {
     for (int j = 0; j < n; ++j) {
       int ni = shells_[i].n_func(), nj = shells_[j].n_func();
       std::vector<double> blk = eri_block(e, i, j, i, j);
@@ -212,6 +215,16 @@ std::vector<double> Basis::schwarz(Engine e) const {
         }
       q[(size_t)i * n + j] = std::sqrt(mx);
     }
+  };
+  int nt = (int)std::thread::hardware_concurrency();
+  if (nt < 1) nt = 1;
+  if (nt > 64) nt = 64;
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; ++t)
+    th.emplace_back([&, t] {
+      for (int i = t; i < n; i += nt) row(i);
+    });
+  for (auto& x : th) x.join();
   return q;
 }
 

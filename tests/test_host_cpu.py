@@ -1,0 +1,141 @@
+"""CPU-side checks of the product: the C-ABI library loads and exports every
+symbol declared in include/integral_gpu.h, argument validation and error
+codes that need no device, the synthetic systems, and the multi-rank
+sharding (world size 2 over gloo)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import integral_b200 as ib
+from integral_b200 import _lib, sharding
+from integral_b200 import systems as S
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "integral_gpu.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|uint32_t|const char\*)\s+(igpu_\w+)\s*\(", txt, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    syms = header_symbols()
+    assert len(syms) >= 18
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(syms) == set(_lib.EXPORTED)
+
+
+def test_abi_version():
+    assert ib.abi_version() == 1
+
+
+def _shell(l=0, nprim=1, exps=(1.0,), coefs=(1.0,)):
+    s = _lib.IgpuShell()
+    s.l = l
+    s.spherical = 0
+    ex = (ctypes.c_double * max(1, len(exps)))(*exps)
+    co = (ctypes.c_double * max(1, len(coefs)))(*coefs)
+    s.nprim = nprim
+    s.exps = ctypes.cast(ex, _lib.c_double_p)
+    s.coefs = ctypes.cast(co, _lib.c_double_p)
+    return s, (ex, co)
+
+
+def test_plan_create_validation_codes():
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    s, keep = _shell(nprim=0)
+    assert L.igpu_plan_create(ctypes.byref(s), 1, 0, ctypes.byref(h)) == -2  # EmptyContraction
+    s, keep = _shell(l=7)
+    assert L.igpu_plan_create(ctypes.byref(s), 1, 0, ctypes.byref(h)) == -4  # AngularMomentumTooHigh
+    s, keep = _shell()
+    assert L.igpu_plan_create(ctypes.byref(s), 1, 5, ctypes.byref(h)) == -1  # unknown engine
+    assert L.igpu_plan_create(ctypes.byref(s), 1, 0, None) == -1
+    assert b"NULL" in L.igpu_last_error_string()
+
+
+def test_python_shell_validation_mirrors_reference():
+    with pytest.raises(ib.IntegralError) as e:
+        ib.Shell(0, [0, 0, 0], [], [])
+    assert e.value.code == -2
+    with pytest.raises(ib.IntegralError) as e:
+        ib.Shell(0, [0, 0, 0], [1.0, 2.0], [1.0])
+    assert e.value.code == -3
+    with pytest.raises(ib.IntegralError) as e:
+        ib.Shell(7, [0, 0, 0], [1.0], [1.0])
+    assert e.value.code == -4
+    s = ib.Shell.new_spherical(3, [0, 0, 0], [1.0], [1.0])
+    assert s.n_func() == 7 and s.n_cart() == 10
+
+
+def test_basis_metadata_without_device():
+    shells = [ib.Shell.from_dict(d) for d in S.direct_grad_fixture(False)]
+    B = ib.Basis(shells)
+    assert B.nao() == 1 + 3 + 6 + 1 + 10 + 3
+    assert B.offsets() == [0, 1, 4, 10, 11, 21]
+    assert len(B.atoms()) == 3
+
+
+def test_synthetic_system_sizes():
+    # AO counts follow the shell lists (Basis::nao), never a quoted figure
+    assert S.nao_of(S.dense_eri_system()["shells"]) == 54
+    assert S.nao_of(S.jk_system()["shells"]) == 960
+    assert S.nao_of(S.jk_spherical_system()["shells"]) == 5200
+    assert S.nao_of(S.grad_system()["shells"]) == 1400
+    a = S.jk_system()
+    b = S.jk_system()
+    assert np.array_equal(a["dens"], b["dens"])
+
+
+def test_bra_shards_partition_the_pairs():
+    nbra = 1000
+    parts = [sharding.bra_shard(nbra, r, 3) for r in range(3)]
+    allp = np.sort(np.concatenate(parts))
+    assert np.array_equal(allp, np.arange(nbra))
+
+
+def _rank_main(rank, world, port, result_path):
+    import sys
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import torch.distributed as dist
+    import oracle_py as O
+    from integral_b200 import sharding as sh
+    from integral_b200 import systems as syst
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world)
+    s = syst.jk_system(natom=5, side=6.0, ndens=2)
+    B = O.OracleBasis(s["shells"])
+    nbra = len(s["shells"]) * (len(s["shells"]) + 1) // 2
+    J, K, cnt, _ = B.direct_jk(s["dens"], 1e-12, bras=sh.bra_shard(nbra, rank, world))
+    counts = np.array([float(cnt)])
+    sh.all_reduce_sum([J, K, counts])
+    if rank == 0:
+        np.savez(result_path, J=J, K=K, count=counts)
+    dist.destroy_process_group()
+
+
+def test_two_rank_sharded_jk_equals_single_rank(tmp_path):
+    """World size 2 over gloo: each rank builds the J/K of its bra shard and
+    one all-reduce sums them; the result equals the unsharded build."""
+    import socket
+
+    import torch.multiprocessing as mp
+    sock = socket.socket()
+    sock.bind(("127.0.0.1", 0))
+    port = sock.getsockname()[1]
+    sock.close()
+    out = str(tmp_path / "r.npz")
+    mp.start_processes(_rank_main, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
+    import oracle_py as O
+    s = S.jk_system(natom=5, side=6.0, ndens=2)
+    B = O.OracleBasis(s["shells"])
+    J, K, cnt, _ = B.direct_jk(s["dens"], 1e-12)
+    r = np.load(out)
+    assert int(r["count"][0]) == cnt
+    assert float(np.max(np.abs(r["J"] - J))) < 1e-12 * float(np.max(np.abs(J)))
+    assert float(np.max(np.abs(r["K"] - K))) < 1e-12 * float(np.max(np.abs(K)))

@@ -1,0 +1,252 @@
+"""CPU checks of the oracle (the C++ restatement of the reference path)
+against the reference's own known answers and golden fixtures.
+
+Mirrors the reference's unit tests: src/math/boys.rs:432-684,
+src/math/rys.rs:574-781, tests/c2s_independent_reference.rs,
+src/math/norm.rs:95-145, tests/two_electron.rs, tests/screening.rs,
+tests/direct_contractor.rs and tests/direct_grad_contractor.rs.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle_py as O
+from integral_b200 import systems as S
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+# ---------------------------------------------------------------- Boys
+
+def test_boys_known_value():
+    # boys.rs:517-520
+    assert abs(O.boys(0, 1.0)[0] - 0.7468241328124271) < 1e-14
+
+
+def test_boys_at_zero_is_inverse_odd():
+    # boys.rs:468-483
+    f = O.boys(24, 0.0)
+    for m in range(25):
+        assert abs(f[m] - 1.0 / (2 * m + 1)) < 1e-15
+
+
+def test_boys_table_matches_reference_path():
+    # boys.rs:485-514: the Taylor table reproduces the series/asymptotic path
+    worst = 0.0
+    for t in np.arange(0.0, 95.0, 0.037):
+        for m in (0, 1, 4, 8, 12, 16, 20, 24):
+            a = O.boys(m, float(t))
+            b = O.boys(m, float(t), reference=True)
+            worst = max(worst, float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300))))
+    assert worst < 1e-12, worst
+
+
+def test_boys_downward_recurrence():
+    for t in (0.3, 2.5, 17.0, 60.0):
+        f = O.boys(10, t)
+        for m in range(1, 11):
+            assert abs(f[m - 1] - (2 * t * f[m] + math.exp(-t)) / (2 * m - 1)) <= 1e-13 * f[m - 1]
+
+
+# ------------------------------------------------------------------ Rys
+
+@pytest.mark.parametrize("n", list(range(1, 14)))
+def test_rys_moments_and_shape(n):
+    # rys.rs:578-626: sum w x^k = F_k(T), roots in (0,1) ascending, w > 0
+    for t in (0.0, 1e-4, 0.5, 2.0, 7.0, 20.0, 45.0, 80.0, 150.0, 1000.0):
+        r, w = O.rys(n, t)
+        fm = O.boys(2 * n - 1, t, reference=True)
+        for k in range(2 * n):
+            q = float(np.sum(w * r ** k))
+            assert abs(q - fm[k]) <= 1e-9 * abs(fm[k]) + 1e-300, (n, t, k)
+        assert np.all(r > 0) and np.all(r < 1) and np.all(w > 0)
+        assert np.all(np.diff(r) > 0)
+
+
+def test_one_point_quadrature_is_mean_and_mass():
+    # rys.rs:648-660
+    for t in (0.0, 0.7, 5.0, 30.0):
+        r, w = O.rys(1, t)
+        f = O.boys(1, t, reference=True)
+        assert abs(r[0] - f[1] / f[0]) < 1e-14 and abs(w[0] - f[0]) < 1e-14
+
+
+def test_rys_table_generator_reproduces_reference_tables():
+    """The restated generator (xtask/src/gen_rys_tables.rs) picks the same
+    subdivision as the reference's committed tables and agrees with their
+    coefficients to the f64 rounding of the generating eigen-solve."""
+    gold = json.load(open(os.path.join(GOLDEN, "rys_tables.json")))["tables"]
+    worst = 0.0
+    for n in range(1, 14):
+        nsub, _, rc, wc = O.rys_table(n, regenerated=True)
+        g = gold[str(n)]
+        assert nsub == g["n_sub"]
+        for mine, ref in ((rc[0], g["root_first"]), (rc[-1], g["root_last"]),
+                          (wc[0], g["weight_first"]), (wc[-1], g["weight_last"])):
+            worst = max(worst, float(np.max(np.abs(np.asarray(mine) - np.asarray(ref)))))
+    assert worst < 5e-15, worst
+
+
+def test_runtime_tables_are_reference_literals_when_built_with_them():
+    import hashlib
+    import struct
+    if not O.lib().orc_rys_tables_are_reference_literals():
+        pytest.skip("oracle built without the extracted reference tables")
+    gold = json.load(open(os.path.join(GOLDEN, "rys_tables.json")))["tables"]
+    for n in range(1, 14):
+        nsub, _, rc, wc = O.rys_table(n, regenerated=False)
+        for arr, key in ((rc, "root_sha256"), (wc, "weight_sha256")):
+            flat = [float(v) for v in np.asarray(arr).reshape(-1)]
+            assert hashlib.sha256(struct.pack("<%dd" % len(flat), *flat)).hexdigest() == gold[str(n)][key]
+
+
+# --------------------------------------------------------- c2s, norms, AM
+
+def test_c2s_matches_signed_mpmath_reference():
+    rows = json.load(open(os.path.join(GOLDEN, "c2s_signed.json")))["rows"]
+    for l in range(5):
+        m = O.c2s(l)
+        ref = np.array(rows[str(l)])
+        assert m.shape == ref.shape
+        assert float(np.max(np.abs(m - ref))) < 1e-12
+
+
+def test_normalized_primitive_has_unit_self_overlap():
+    # norm.rs:95-145
+    def df(n):
+        a = 1.0
+        while n > 1:
+            a *= n
+            n -= 2
+        return a
+    for alpha in (0.1, 0.8, 3.3, 25.0, 1e5):
+        for lx, ly, lz in ((0, 0, 0), (1, 0, 0), (0, 1, 1), (2, 0, 0), (1, 1, 1), (3, 2, 1)):
+            n = O.cart_norm(alpha, lx, ly, lz)
+            L = lx + ly + lz
+            raw = df(2 * lx - 1) * df(2 * ly - 1) * df(2 * lz - 1) / (4 * alpha) ** L * (math.pi / (2 * alpha)) ** 1.5
+            assert abs(n * n * raw - 1.0) < 1e-12
+
+
+def test_select_engine_bands():
+    # integrals.rs:374-388 and tests/dispatch.rs
+    assert O.select_engine(2, 3, 1) == "os"
+    assert O.select_engine(3, 3, 2) == "rys"
+    assert O.select_engine(3, 3, 3) == "os"
+    assert O.select_engine(8, 2, 15) == "rys"
+    assert O.select_engine(8, 2, 16) == "os"
+    assert O.select_engine(9, 8, 10000) == "rys"
+
+
+# ------------------------------------------------------------------ ERIs
+
+@pytest.fixture(scope="module", params=[False, True], ids=["cart", "sph"])
+def fixture_basis(request):
+    shells = S.direct_contractor_fixture(request.param)
+    return O.OracleBasis(shells)
+
+
+def test_os_and_rys_agree(fixture_basis):
+    # tests/cross_engine.rs: the two engines agree to 1e-11
+    a = fixture_basis.eri("os")
+    b = fixture_basis.eri("rys")
+    peak = float(np.max(np.abs(a)))
+    assert float(np.max(np.abs(a - b))) < 1e-11 * max(peak, 1.0)
+
+
+def test_eightfold_symmetry(fixture_basis):
+    n = fixture_basis.nao
+    T = fixture_basis.eri().reshape(n, n, n, n)
+    for perm in ((1, 0, 2, 3), (0, 1, 3, 2), (2, 3, 0, 1), (3, 2, 1, 0)):
+        assert float(np.max(np.abs(T - T.transpose(perm)))) < 1e-13
+
+
+def test_schwarz_bounds_every_element(fixture_basis):
+    # tests/screening.rs: |(mu nu|la si)| <= Q_ij Q_kl
+    shells = fixture_basis.shells
+    q = fixture_basis.schwarz()
+    n = len(shells)
+    for i in range(n):
+        for j in range(n):
+            for k in range(n):
+                for l in range(n):
+                    blk = fixture_basis.eri_block(i, j, k, l)
+                    assert float(np.max(np.abs(blk))) <= q[i, j] * q[k, l] * (1 + 1e-12) + 1e-300
+
+
+def test_direct_jk_matches_dense_contraction(fixture_basis):
+    # tests/direct_contractor.rs: threshold 0, two densities, max |dJK| < 1e-9
+    n = fixture_basis.nao
+    D = S.direct_contractor_densities(n)
+    for engine in ("os", "rys"):
+        J, K, _, _ = fixture_basis.direct_jk(D, 0.0, engine=engine)
+        E = fixture_basis.eri(engine).reshape(n, n, n, n)
+        for d in range(2):
+            Jr = np.einsum("abcd,cd->ab", E, D[d])
+            Kr = np.einsum("abcd,bd->ac", E, D[d])
+            assert float(np.max(np.abs(J[d] - Jr))) < 1e-9
+            assert float(np.max(np.abs(K[d] - Kr))) < 1e-9
+
+
+def test_direct_jk_threads_match_serial():
+    sh = S.jk_system(natom=6, side=7.0)
+    B = O.OracleBasis(sh["shells"])
+    J1, K1, c1, h1 = B.direct_jk(sh["dens"], 1e-12, nthreads=1)
+    J4, K4, c4, h4 = B.direct_jk(sh["dens"], 1e-12, nthreads=4)
+    assert (c1, h1) == (c4, h4)
+    # only the summation order of the per-worker buffers differs
+    assert float(np.max(np.abs(J1 - J4))) < 1e-13 * float(np.max(np.abs(J1)))
+    assert float(np.max(np.abs(K1 - K4))) < 1e-13 * float(np.max(np.abs(K1)))
+
+
+# -------------------------------------------------------------- gradient
+
+def _dense_energy(basis, coulomb, exchange):
+    n = basis.nao
+    E = basis.eri().reshape(n, n, n, n)
+    e = 0.0
+    for f, L, R in coulomb:
+        e += f * np.einsum("pq,pqrs,rs->", L, E, R)
+    for f, L, R in exchange:
+        e += f * np.einsum("pr,pqrs,qs->", L, E, R)
+    return e
+
+
+@pytest.mark.parametrize("spherical", [False, True])
+def test_direct_gradient_matches_finite_difference(spherical):
+    # tests/direct_grad_contractor.rs: central FD at h = 2e-4, tolerance 1e-6
+    shells = S.direct_grad_fixture(spherical)
+    B = O.OracleBasis(shells)
+    n = B.nao
+    coul, exch = S.grad_fixture_terms(n)
+    g, _, _ = B.direct_grad(coul, exch, 0.0)
+    # zero net force
+    assert float(np.max(np.abs(g.sum(axis=0)))) < 1e-10
+    h = 2e-4
+    atoms = []
+    for s in shells:
+        if s["center"] not in atoms:
+            atoms.append(s["center"])
+    for a in range(len(atoms)):
+        for x in range(3):
+            vals = []
+            for sgn in (+1, -1):
+                moved = []
+                for s in shells:
+                    c = list(s["center"])
+                    if s["center"] == atoms[a]:
+                        c[x] += sgn * h
+                    moved.append(dict(s, center=c))
+                vals.append(_dense_energy(O.OracleBasis(moved), coul, exch))
+            fd = (vals[0] - vals[1]) / (2 * h)
+            assert abs(fd - g[a, x]) < 1e-6, (a, x, fd, g[a, x])
+
+
+def test_gradient_single_atom_is_zero():
+    shells = [dict(s, center=[0.1, -0.2, 0.3]) for s in S.direct_grad_fixture(False)]
+    B = O.OracleBasis(shells)
+    coul, exch = S.grad_fixture_terms(B.nao)
+    g, cnt, _ = B.direct_grad(coul, exch, 0.0)
+    assert cnt == 0 and float(np.max(np.abs(g))) == 0.0
