@@ -107,21 +107,25 @@ struct JKDev {
   double threshold;
 };
 
+// Two-particle density of the gradient as product terms factor * L (x) R
+// (GradDensityTerm, src/direct_grad.rs:21-25).  Per term: device pointers to
+// the nao x nao matrices and to their symmetrised shell-block maxima
+// (nsh x nsh, src/direct_grad.rs:292-312).  c* = Coulomb-type terms, x* =
+// exchange-type terms.
 struct GradDev {
-  // term matrices: nterm x nao x nao for left and right
-  const double* cl;
-  const double* cr;
+  const double* const* cl;
+  const double* const* cr;
+  const double* const* cl_max;
+  const double* const* cr_max;
   const double* cf;      // factors
-  const double* xl;
-  const double* xr;
+  const double* const* xl;
+  const double* const* xr;
+  const double* const* xl_max;
+  const double* const* xr_max;
   const double* xf;
-  const double* cl_max;  // per term symmetrised shell-block maxima nsh x nsh
-  const double* cr_max;
-  const double* xl_max;
-  const double* xr_max;
   int ncoul, nexch;
   double threshold;
-  double* out;           // natom x 3
+  double* out;           // natom x 3, dE/dR accumulated
 };
 
 struct Counters {

@@ -35,6 +35,31 @@ IGPU_DECL(13)
 IGPU_DECL(14)
 #endif
 
+#define IGPU_GDECL(n)                                         \
+  void register_grad_classes_##n(KernelEntry* tab, int npc); \
+  cudaError_t upload_grad_constants_##n(const ConstData& c);
+IGPU_GDECL(0)
+IGPU_GDECL(1)
+IGPU_GDECL(2)
+#if GRAD_KERNEL_MAX_L >= 2
+IGPU_GDECL(3)
+IGPU_GDECL(4)
+IGPU_GDECL(5)
+#endif
+#if GRAD_KERNEL_MAX_L >= 3
+IGPU_GDECL(6)
+IGPU_GDECL(7)
+IGPU_GDECL(8)
+IGPU_GDECL(9)
+#endif
+#if GRAD_KERNEL_MAX_L >= 4
+IGPU_GDECL(10)
+IGPU_GDECL(11)
+IGPU_GDECL(12)
+IGPU_GDECL(13)
+IGPU_GDECL(14)
+#endif
+
 using RegFn = void (*)(KernelEntry*, int);
 using UpFn = cudaError_t (*)(const ConstData&);
 static const RegFn k_reg[NPC] = {
@@ -58,21 +83,63 @@ static const UpFn k_up[NPC] = {
 #endif
 };
 
+constexpr int GNPC = (GRAD_KERNEL_MAX_L + 1) * (GRAD_KERNEL_MAX_L + 2) / 2;
+static const RegFn g_reg[GNPC] = {
+    register_grad_classes_0, register_grad_classes_1, register_grad_classes_2,
+#if GRAD_KERNEL_MAX_L >= 2
+    register_grad_classes_3, register_grad_classes_4, register_grad_classes_5,
+#endif
+#if GRAD_KERNEL_MAX_L >= 3
+    register_grad_classes_6, register_grad_classes_7, register_grad_classes_8, register_grad_classes_9,
+#endif
+#if GRAD_KERNEL_MAX_L >= 4
+    register_grad_classes_10, register_grad_classes_11, register_grad_classes_12, register_grad_classes_13,
+    register_grad_classes_14,
+#endif
+};
+static const UpFn g_up[GNPC] = {
+    upload_grad_constants_0, upload_grad_constants_1, upload_grad_constants_2,
+#if GRAD_KERNEL_MAX_L >= 2
+    upload_grad_constants_3, upload_grad_constants_4, upload_grad_constants_5,
+#endif
+#if GRAD_KERNEL_MAX_L >= 3
+    upload_grad_constants_6, upload_grad_constants_7, upload_grad_constants_8, upload_grad_constants_9,
+#endif
+#if GRAD_KERNEL_MAX_L >= 4
+    upload_grad_constants_10, upload_grad_constants_11, upload_grad_constants_12, upload_grad_constants_13,
+    upload_grad_constants_14,
+#endif
+};
+
 static KernelEntry g_table[NPC * NPC];
-static std::once_flag g_once;
+static KernelEntry g_grad_table[GNPC * GNPC];
+static std::once_flag g_once, g_grad_once;
 
 int kernel_npc() { return NPC; }
+
+static void set_smem_limits(KernelEntry* tab, int n) {
+  for (int q = 0; q < n; ++q) {
+    KernelEntry& e = tab[q];
+    if (!e.valid) continue;
+    cudaFuncSetAttribute(reinterpret_cast<const void*>(e.k64), cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem64);
+    cudaFuncSetAttribute(reinterpret_cast<const void*>(e.k32), cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem32);
+  }
+}
+
+const KernelEntry* grad_entry(int pcb, int pck) {
+  std::call_once(g_grad_once, [] {
+    for (int b = 0; b < GNPC; ++b) g_reg[b](g_grad_table, GNPC);
+    set_smem_limits(g_grad_table, GNPC * GNPC);
+  });
+  if (pcb < 0 || pck < 0 || pcb >= GNPC || pck >= GNPC || pcb < pck) return nullptr;
+  const KernelEntry* e = &g_grad_table[pcb * GNPC + pck];
+  return e->valid ? e : nullptr;
+}
 
 const KernelEntry* kernel_entry(int pcb, int pck) {
   std::call_once(g_once, [] {
     for (int b = 0; b < NPC; ++b) k_reg[b](g_table, NPC);
-    for (auto& e : g_table) {
-      if (!e.valid) continue;
-      cudaFuncSetAttribute(reinterpret_cast<const void*>(e.k64), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           e.smem64);
-      cudaFuncSetAttribute(reinterpret_cast<const void*>(e.k32), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           e.smem32);
-    }
+    set_smem_limits(g_table, NPC * NPC);
   });
   if (pcb < 0 || pck < 0 || pcb >= NPC || pck >= NPC || pcb < pck) return nullptr;
   const KernelEntry* e = &g_table[pcb * NPC + pck];
@@ -82,6 +149,10 @@ const KernelEntry* kernel_entry(int pcb, int pck) {
 cudaError_t upload_all_constants(const ConstData& c) {
   for (int b = 0; b < NPC; ++b) {
     cudaError_t e = k_up[b](c);
+    if (e != cudaSuccess) return e;
+  }
+  for (int b = 0; b < GNPC; ++b) {
+    cudaError_t e = g_up[b](c);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

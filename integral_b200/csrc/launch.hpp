@@ -21,7 +21,15 @@ struct KernelEntry {
   bool valid = false;
 };
 
+// Highest shell l of the compiled gradient classes.
+#ifndef GRAD_KERNEL_MAX_L
+#define GRAD_KERNEL_MAX_L 3
+#endif
+
 int kernel_npc();
+// Gradient kernel of the class (pcb | pck), same conventions; the entry's
+// slot is the gradient scratch per team.
+const KernelEntry* grad_entry(int pcb, int pck);
 // Entry of the class (pcb | pck), pair classes pc = l_a(l_a+1)/2 + l_b with
 // l_a >= l_b and pcb >= pck; nullptr when the class is not compiled.
 const KernelEntry* kernel_entry(int pcb, int pck);

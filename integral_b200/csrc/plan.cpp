@@ -24,7 +24,6 @@
 #include <vector>
 
 #include "../../include/integral_gpu.h"
-#include "grad.hpp"
 #include "host_math.hpp"
 #include "launch.hpp"
 
@@ -137,7 +136,9 @@ struct igpu_plan {
   std::vector<cudaEvent_t> events;
   std::vector<igpu_launch_record> profile;
   std::vector<size_t> profile_launch;
-  GradState grad;
+  // gradient: term matrices, their block maxima and the device term tables
+  DevBuf<double> d_gmat, d_gmax, d_gfac, d_gout;
+  DevBuf<const double*> d_gptr;
 };
 
 namespace {
@@ -240,6 +241,27 @@ double model_flops_quartet(int la, int lb, int lc, int ld, bool sph, int ndens, 
   if (jk) f += 4.0 * 8.0 * dims[0] * dims[1] * dims[2] * dims[3] * ndens;
   return f;
 }
+// Gradient per primitive quartet: the reference's three raised and up to
+// three lowered shifted classes (src/direct_grad.rs:431-470), each at the
+// value model above.
+double model_flops_grad_prim(int la, int lb, int lc, int ld) {
+  double f = model_flops_prim(la + 1, lb, lc, ld) + model_flops_prim(la, lb + 1, lc, ld) +
+             model_flops_prim(la, lb, lc + 1, ld);
+  if (la > 0) f += model_flops_prim(la - 1, lb, lc, ld);
+  if (lb > 0) f += model_flops_prim(la, lb - 1, lc, ld);
+  if (lc > 0) f += model_flops_prim(la, lb, lc - 1, ld);
+  return f;
+}
+// Gradient per shell quartet: the weight block (4 flops per Coulomb term and
+// 10 per exchange term and element), its pull-back to Cartesian, and the
+// dots of W with the six shifted blocks on three axes.
+double model_flops_grad_quartet(int la, int lb, int lc, int ld, bool sph, int nterm_c, int nterm_x) {
+  auto nc = [](int l) { return (double)((l + 1) * (l + 2) / 2); };
+  const double W = nc(la) * nc(lb) * nc(lc) * nc(ld);
+  double f = W * (4.0 * nterm_c + 10.0 * nterm_x) + 6.0 * 3.0 * 2.0 * W;
+  if (sph) f += model_flops_quartet(la, lb, lc, ld, true, 0, false);
+  return f;
+}
 
 // Scratch doubles per team: the class slot plus, for symmetric J/K, the
 // running bra-block accumulators (bra index + ndens blocks of the bra pair).
@@ -253,10 +275,12 @@ size_t slot_with_acc(const KernelEntry* e, int pcb, const KernelArgs& A) {
 // Run every launch of a task set; quartet kernels only.  Per-launch device
 // time and counters are kept for igpu_last_profile.
 int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t& launches) {
+  const bool grad = A.mode == MODE_GRAD;
+  auto entry = [grad](int pcb, int pck) { return grad ? grad_entry(pcb, pck) : kernel_entry(pcb, pck); };
   size_t need = 0;
   for (auto& L : ts.launches) {
     if (L->total == 0) continue;
-    const KernelEntry* e = kernel_entry(L->pcb, L->pck);
+    const KernelEntry* e = entry(L->pcb, L->pck);
     if (!e) return fail(IGPU_ERR_UNSUPPORTED, "angular class not compiled for the GPU");
     need = std::max(need, grid_for(e, L->fp32, L->total) * (128 / e->team) * slot_with_acc(e, L->pcb, A));
   }
@@ -276,7 +300,7 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
   for (size_t li = 0; li < nl; ++li) {
     Launch* L = ts.launches[li].get();
     if (L->total == 0) continue;
-    const KernelEntry* e = kernel_entry(L->pcb, L->pck);
+    const KernelEntry* e = entry(L->pcb, L->pck);
     const size_t grid = grid_for(e, L->fp32, L->total);
     A.scratch = P->d_scratch.p;
     A.slot_doubles = slot_with_acc(e, L->pcb, A);
@@ -312,7 +336,7 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
 }
 
 // After the stream is synchronised: per-launch times, counters, model flops.
-int collect_profile(igpu_plan* P, int ndens, bool jk) {
+int collect_profile(igpu_plan* P, int ndens, bool jk, int grad_terms_c = -1, int grad_terms_x = 0) {
   const size_t nl = P->profile.empty() ? 0 : P->profile_launch.back() + 1;
   std::vector<Counters> c(nl);
   if (nl) CK(cudaMemcpy(c.data(), P->d_launch_counters.p, nl * sizeof(Counters), cudaMemcpyDeviceToHost));
@@ -325,8 +349,13 @@ int collect_profile(igpu_plan* P, int ndens, bool jk) {
     r.ms = ms;
     r.quartets = c[li].quartets;
     r.prim_quartets = c[li].prim_quartets;
-    r.model_flops = (double)r.prim_quartets * model_flops_prim(r.la, r.lb, r.lc, r.ld) +
-                    (double)r.quartets * model_flops_quartet(r.la, r.lb, r.lc, r.ld, P->all_spherical, ndens, jk);
+    if (grad_terms_c >= 0)
+      r.model_flops = (double)r.prim_quartets * model_flops_grad_prim(r.la, r.lb, r.lc, r.ld) +
+                      (double)r.quartets * model_flops_grad_quartet(r.la, r.lb, r.lc, r.ld, P->all_spherical,
+                                                                    grad_terms_c, grad_terms_x);
+    else
+      r.model_flops = (double)r.prim_quartets * model_flops_prim(r.la, r.lb, r.lc, r.ld) +
+                      (double)r.quartets * model_flops_quartet(r.la, r.lb, r.lc, r.ld, P->all_spherical, ndens, jk);
     P->last.quartets += c[li].quartets;
     P->last.quartet_hash += c[li].hash;
     P->last.quartets_fp32 += c[li].fp32_quartets;
@@ -613,8 +642,6 @@ int igpu_plan_create(const igpu_shell* sh, size_t nsh, int engine, igpu_plan** o
       P->class_pairs[pr.cls].push_back((int)P->pairs.size() - 1);
     }
   P->npairs = (int)P->pairs.size();
-  P->grad.expv = expv;
-  P->grad.eff = eff;
   CK(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
   CK(cudaEventCreate(&P->ev0));
   CK(cudaEventCreate(&P->ev1));
@@ -935,15 +962,171 @@ int igpu_last_profile(const igpu_plan* P, igpu_launch_record* out, size_t cap, s
   return IGPU_OK;
 }
 
-int igpu_grad(igpu_plan* P, const igpu_term* coulomb, int ncoul, const igpu_term* exchange, int nexch,
-              const uint32_t* bra_subset, size_t nsub, double threshold, int precision, double* out) {
-  return grad_host(P, coulomb, ncoul, exchange, nexch, bra_subset, nsub, threshold, precision, out);
-}
-
-int igpu_grad_device(igpu_plan* P, const igpu_term* d_coulomb, int ncoul, const igpu_term* d_exchange, int nexch,
+int igpu_grad_device(igpu_plan* P, const igpu_term* coulomb, int ncoul, const igpu_term* exchange, int nexch,
                      const uint32_t* bra_subset, size_t nsub, double threshold, int precision, double* d_out,
                      void* stream) {
-  return grad_device(P, d_coulomb, ncoul, d_exchange, nexch, bra_subset, nsub, threshold, precision, d_out, stream);
+  if (!P || !d_out) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (ncoul < 0 || nexch < 0 || (ncoul > 0 && !coulomb) || (nexch > 0 && !exchange))
+    return fail(IGPU_ERR_INVALID_ARGUMENT, "invalid term list");
+  for (int t = 0; t < ncoul; ++t)
+    if (!coulomb[t].left || !coulomb[t].right) return fail(IGPU_ERR_INVALID_ARGUMENT, "term matrix is NULL");
+  for (int t = 0; t < nexch; ++t)
+    if (!exchange[t].left || !exchange[t].right) return fail(IGPU_ERR_INVALID_ARGUMENT, "term matrix is NULL");
+  if (precision != IGPU_PRECISION_FP64 && precision != IGPU_PRECISION_MIXED)
+    return fail(IGPU_ERR_INVALID_ARGUMENT, "unknown precision");
+  if (std::isnan(threshold)) return fail(IGPU_ERR_INVALID_ARGUMENT, "threshold is NaN");
+  // DirectGradContractor::new (src/direct_grad.rs:181-186)
+  for (const DevShell& d : P->shells) {
+    if (d.l > MAX_GRAD_L)
+      return fail(IGPU_ERR_ANGULAR_MOMENTUM_GRAD, "angular momentum too high for the gradient (l <= 5)");
+    if (d.l > GRAD_KERNEL_MAX_L)
+      return fail(IGPU_ERR_UNSUPPORTED, "shell angular momentum above the compiled gradient classes (l <= " +
+                                            std::to_string(GRAD_KERNEL_MAX_L) + ")");
+  }
+  cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
+  std::vector<unsigned> bitmap;
+  if (bra_subset) {
+    int rc = check_bra_subset(P, bra_subset, nsub, bitmap);
+    if (rc) return rc;
+    CK(P->d_bitmap.ensure(bitmap.size()));
+    CK(cudaMemcpyAsync(P->d_bitmap.p, bitmap.data(), bitmap.size() * sizeof(unsigned), cudaMemcpyHostToDevice, s));
+  }
+  // symmetrised shell-block maxima of every distinct matrix (direct_grad.rs:
+  // 272-312), one pass per matrix
+  std::vector<const double*> mats;
+  auto index_of = [&mats](const double* m) {
+    for (size_t q = 0; q < mats.size(); ++q)
+      if (mats[q] == m) return (int)q;
+    mats.push_back(m);
+    return (int)mats.size() - 1;
+  };
+  std::vector<int> ci(2 * ncoul), xi(2 * nexch);
+  for (int t = 0; t < ncoul; ++t) {
+    ci[2 * t] = index_of(coulomb[t].left);
+    ci[2 * t + 1] = index_of(coulomb[t].right);
+  }
+  for (int t = 0; t < nexch; ++t) {
+    xi[2 * t] = index_of(exchange[t].left);
+    xi[2 * t + 1] = index_of(exchange[t].right);
+  }
+  const size_t nn = (size_t)P->nsh * P->nsh;
+  CK(P->d_gmax.ensure(nn * std::max<size_t>(1, mats.size())));
+  for (size_t m = 0; m < mats.size(); ++m)
+    CK(launch_shell_block_max(mats[m], 1, P->d_shells.p, P->nsh, P->nao, 1, P->d_gmax.p + m * nn, s));
+  // pointer table: cl, cr, cl_max, cr_max (ncoul each), then xl, xr, xl_max, xr_max
+  std::vector<const double*> ptr(4 * (size_t)ncoul + 4 * (size_t)nexch);
+  std::vector<double> fac(ncoul + nexch);
+  for (int t = 0; t < ncoul; ++t) {
+    ptr[t] = coulomb[t].left;
+    ptr[ncoul + t] = coulomb[t].right;
+    ptr[2 * ncoul + t] = P->d_gmax.p + ci[2 * t] * nn;
+    ptr[3 * ncoul + t] = P->d_gmax.p + ci[2 * t + 1] * nn;
+    fac[t] = coulomb[t].factor;
+  }
+  const size_t xo = 4 * (size_t)ncoul;
+  for (int t = 0; t < nexch; ++t) {
+    ptr[xo + t] = exchange[t].left;
+    ptr[xo + nexch + t] = exchange[t].right;
+    ptr[xo + 2 * nexch + t] = P->d_gmax.p + xi[2 * t] * nn;
+    ptr[xo + 3 * nexch + t] = P->d_gmax.p + xi[2 * t + 1] * nn;
+    fac[ncoul + t] = exchange[t].factor;
+  }
+  CK(P->d_gptr.ensure(ptr.size()));
+  if (!ptr.empty())
+    CK(cudaMemcpyAsync(P->d_gptr.p, ptr.data(), ptr.size() * sizeof(const double*), cudaMemcpyHostToDevice, s));
+  CK(P->d_gfac.ensure(fac.size()));
+  if (!fac.empty())
+    CK(cudaMemcpyAsync(P->d_gfac.p, fac.data(), fac.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  // FP64 part of MIXED: Q_bra*Q_ket*max|block| >= cutoff
+  double fp64_cut = 0.0;
+  if (precision == IGPU_PRECISION_MIXED) {
+    std::vector<double> hb(nn * mats.size());
+    if (!hb.empty())
+      CK(cudaMemcpyAsync(hb.data(), P->d_gmax.p, hb.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    double dmax = 0.0;
+    for (double v : hb) dmax = std::max(dmax, v);
+    fp64_cut = dmax > 0.0 ? P->mixed_cutoff / dmax : std::numeric_limits<double>::infinity();
+    if (fp64_cut <= 0.0) fp64_cut = std::numeric_limits<double>::min();
+  } else {
+    CK(cudaStreamSynchronize(s));
+  }
+  auto key = std::make_pair(threshold, fp64_cut);
+  auto it = P->jk_tasks.find(key);
+  if (it == P->jk_tasks.end()) {
+    auto ts = std::make_unique<TaskSet>();
+    int rc = build_jk_tasks(P, threshold, fp64_cut, *ts);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(P->stream));
+    it = P->jk_tasks.emplace(key, std::move(ts)).first;
+  }
+  KernelArgs A = base_args(P);
+  A.mode = MODE_GRAD;
+  const double* const* dp = P->d_gptr.p;
+  A.grad.cl = dp;
+  A.grad.cr = dp + ncoul;
+  A.grad.cl_max = dp + 2 * ncoul;
+  A.grad.cr_max = dp + 3 * ncoul;
+  A.grad.cf = P->d_gfac.p;
+  A.grad.xl = dp + xo;
+  A.grad.xr = dp + xo + nexch;
+  A.grad.xl_max = dp + xo + 2 * nexch;
+  A.grad.xr_max = dp + xo + 3 * nexch;
+  A.grad.xf = P->d_gfac.p + ncoul;
+  A.grad.ncoul = ncoul;
+  A.grad.nexch = nexch;
+  A.grad.threshold = threshold;
+  A.grad.out = d_out;
+  A.bra_bitmap = bra_subset ? P->d_bitmap.p : nullptr;
+  uint32_t launches = (uint32_t)mats.size();
+  int rc = run_tasks(P, *it->second, A, s, launches);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s));
+  return collect_profile(P, 0, false, ncoul, nexch);
+}
+
+int igpu_grad(igpu_plan* P, const igpu_term* coulomb, int ncoul, const igpu_term* exchange, int nexch,
+              const uint32_t* bra_subset, size_t nsub, double threshold, int precision, double* out) {
+  if (!P || !out) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (ncoul < 0 || nexch < 0 || (ncoul > 0 && !coulomb) || (nexch > 0 && !exchange))
+    return fail(IGPU_ERR_INVALID_ARGUMENT, "invalid term list");
+  // distinct host matrices to the device once each
+  std::vector<const double*> host;
+  auto index_of = [&host](const double* m) {
+    for (size_t q = 0; q < host.size(); ++q)
+      if (host[q] == m) return (int)q;
+    host.push_back(m);
+    return (int)host.size() - 1;
+  };
+  std::vector<igpu_term> dc(coulomb, coulomb + ncoul), dx(exchange, exchange + nexch);
+  std::vector<int> idx;
+  for (auto* v : {&dc, &dx})
+    for (auto& t : *v) {
+      if (!t.left || !t.right) return fail(IGPU_ERR_INVALID_ARGUMENT, "term matrix is NULL");
+      idx.push_back(index_of(t.left));
+      idx.push_back(index_of(t.right));
+    }
+  const size_t n2 = (size_t)P->nao * P->nao;
+  CK(P->d_gmat.ensure(n2 * std::max<size_t>(1, host.size())));
+  for (size_t m = 0; m < host.size(); ++m)
+    CK(cudaMemcpyAsync(P->d_gmat.p + m * n2, host[m], n2 * sizeof(double), cudaMemcpyHostToDevice, P->stream));
+  size_t q = 0;
+  for (auto* v : {&dc, &dx})
+    for (auto& t : *v) {
+      t.left = P->d_gmat.p + idx[q++] * n2;
+      t.right = P->d_gmat.p + idx[q++] * n2;
+    }
+  const size_t no = (size_t)P->natom * 3;
+  CK(P->d_gout.ensure(no));
+  CK(cudaMemsetAsync(P->d_gout.p, 0, no * sizeof(double), P->stream));
+  int rc = igpu_grad_device(P, dc.data(), ncoul, dx.data(), nexch, bra_subset, nsub, threshold, precision,
+                            P->d_gout.p, P->stream);
+  if (rc) return rc;
+  std::vector<double> g(no);
+  CK(cudaMemcpyAsync(g.data(), P->d_gout.p, no * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
+  CK(cudaStreamSynchronize(P->stream));
+  for (size_t e = 0; e < no; ++e) out[e] += g[e];
+  return IGPU_OK;
 }
 
 }  // extern "C"

@@ -58,7 +58,32 @@ struct Screen {
   bool swapped;       // reference bra is the evaluation ket pair
   uint64_t mask;      // densities this quartet contributes to
   int i, j, k, l;     // reference canonical shells
+  double degeneracy;  // gradient: images of the canonical quartet
 };
+
+// Bound on the permutation-averaged two-particle density over the function
+// block of canonical quartet (i,j,k,l) (src/direct_grad.rs:626-644).  The
+// rounding of every product and sum is the reference's (no contraction into
+// fused multiply-adds), so the screened list is bit-identical.
+__device__ __forceinline__ double grad_block_bound(const GradDev& g, int nsh, int i, int j, int k, int l) {
+  auto at = [nsh](const double* m, int a, int b) { return __ldg(m + (size_t)a * nsh + b); };
+  double bound = 0.0;
+  for (int t = 0; t < g.ncoul; ++t) {
+    const double* L = g.cl_max[t];
+    const double* R = g.cr_max[t];
+    const double s = __dadd_rn(__dmul_rn(at(L, i, j), at(R, k, l)), __dmul_rn(at(L, k, l), at(R, i, j)));
+    bound = __dadd_rn(bound, __dmul_rn(__dmul_rn(0.5, fabs(g.cf[t])), s));
+  }
+  for (int t = 0; t < g.nexch; ++t) {
+    const double* L = g.xl_max[t];
+    const double* R = g.xr_max[t];
+    double s = __dadd_rn(__dmul_rn(at(L, i, k), at(R, j, l)), __dmul_rn(at(L, j, k), at(R, i, l)));
+    s = __dadd_rn(s, __dmul_rn(at(L, i, l), at(R, j, k)));
+    s = __dadd_rn(s, __dmul_rn(at(L, j, l), at(R, i, k)));
+    bound = __dadd_rn(bound, __dmul_rn(__dmul_rn(0.25, fabs(g.xf[t])), s));
+  }
+  return bound;
+}
 
 // Reference screening of one canonical quartet.  The reference bra is the
 // pair with the larger canonical index (its loops run k <= i, l <= l_top,
@@ -76,6 +101,7 @@ __device__ __forceinline__ Screen screen_quartet(const KernelArgs& A, const Pair
   s.l = rk.j;
   s.mask = 1;
   s.keep = true;
+  s.degeneracy = 1.0;
   if (A.bra_bitmap && !((__ldg(A.bra_bitmap + (rb.tri >> 5)) >> (rb.tri & 31)) & 1u)) {
     s.keep = false;
     return s;
@@ -104,6 +130,28 @@ __device__ __forceinline__ Screen screen_quartet(const KernelArgs& A, const Pair
     }
     s.mask = mask;
     s.keep = mask != 0;
+  } else if (A.mode == MODE_GRAD) {
+    // src/direct_grad.rs:347-370
+    const double thr = A.grad.threshold;
+    const double qab = rb.q;
+    if (qab == 0.0 && thr > 0.0) {
+      s.keep = false;
+      return s;
+    }
+    const int ai = A.shells[s.i].atom, aj = A.shells[s.j].atom, ak = A.shells[s.k].atom, al = A.shells[s.l].atom;
+    if (ai == aj && aj == ak && ak == al) {
+      s.keep = false;
+      return s;
+    }
+    const double pair_bound = qab * rk.q;
+    if (pair_bound < thr) {
+      s.keep = false;
+      return s;
+    }
+    const double deg = (s.i == s.j ? 1.0 : 2.0) * (s.k == s.l ? 1.0 : 2.0) * (s.i == s.k && s.j == s.l ? 1.0 : 2.0);
+    s.degeneracy = deg;
+    if (__dmul_rn(__dmul_rn(pair_bound, deg), grad_block_bound(A.grad, A.nsh, s.i, s.j, s.k, s.l)) < thr)
+      s.keep = false;
   }
   return s;
 }
