@@ -156,6 +156,23 @@ int igpu_jk_device(igpu_plan* plan, const double* d_dens, int ndens, const uint3
                    size_t nsub, double threshold, int want_k, int precision, double* d_J,
                    double* d_K, void* stream);
 
+/* Allocation-free variant of igpu_jk_device (no counterpart in the
+ * reference; added for callers that capture the build in a CUDA graph or
+ * must not allocate): FP64, every canonical bra pair, J += and K +=
+ * directly (any density, symmetric or not).  Its team scratch (64 MiB),
+ * density bounds (ndens * nsh^2 <= 2^21 doubles) and work counters live in
+ * file-scope device storage whose addresses are resolved once per device;
+ * the call makes no cudaMalloc/cudaFree, no host synchronisation and only
+ * memset + kernel launches on `stream`.  Preconditions: the FP64 task list
+ * of `threshold` exists (one earlier igpu_jk or igpu_jk_device call on this
+ * plan with the same threshold), and the first igpu_jk_device_static call
+ * on each device happens outside stream capture.  Oversize requests return
+ * IGPU_ERR_UNSUPPORTED.  The storage is shared by every plan on the device:
+ * calls must be ordered (one stream), never concurrent.  Does not update
+ * igpu_last_stats / igpu_last_profile. */
+int igpu_jk_device_static(igpu_plan* plan, const double* d_dens, int ndens, double threshold, int want_k,
+                          double* d_J, double* d_K, void* stream);
+
 /* DirectGradContractor::density + accumulate_bra_pair / contract
  * (direct_grad.rs:272-392): out[natom][3] += dE/dR.  Host buffers. */
 int igpu_grad(igpu_plan* plan, const igpu_term* coulomb, int ncoul, const igpu_term* exchange,

@@ -392,6 +392,14 @@ class DirectContractor:
             float(threshold), int(bool(want_exchange)), int(precision), ctypes.c_void_p(d_J),
             ctypes.c_void_p(d_K if want_exchange else 0), ctypes.c_void_p(stream or 0)))
 
+    def jk_device_static(self, d_dens, ndens, d_J, d_K, threshold, want_exchange=True, stream=None):
+        """Allocation-free FP64 J/K on device pointers (igpu_jk_device_static):
+        needs one earlier jk/jk_device call with the same threshold; adds into
+        J and K without synchronising the stream."""
+        _lib.check(_lib.lib().igpu_jk_device_static(
+            self._plan.h, ctypes.c_void_p(d_dens), ndens, float(threshold), int(bool(want_exchange)),
+            ctypes.c_void_p(d_J), ctypes.c_void_p(d_K if want_exchange else 0), ctypes.c_void_p(stream or 0)))
+
     def last_stats(self) -> dict:
         return self._plan.stats()
 

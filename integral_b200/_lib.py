@@ -74,6 +74,7 @@ def lib():
                           ctypes.c_int, ctypes.c_int, c_double_p, c_double_p]
     L.igpu_jk_device.argtypes = [vp, vp, ctypes.c_int, c_u32_p, ctypes.c_size_t, ctypes.c_double,
                                  ctypes.c_int, ctypes.c_int, vp, vp, vp]
+    L.igpu_jk_device_static.argtypes = [vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, vp, vp, vp]
     L.igpu_grad.argtypes = [vp, ctypes.POINTER(IgpuTerm), ctypes.c_int, ctypes.POINTER(IgpuTerm), ctypes.c_int,
                             c_u32_p, ctypes.c_size_t, ctypes.c_double, ctypes.c_int, c_double_p]
     L.igpu_grad_device.argtypes = [vp, ctypes.POINTER(IgpuTerm), ctypes.c_int, ctypes.POINTER(IgpuTerm),
@@ -87,7 +88,8 @@ def lib():
 EXPORTED = [
     "igpu_abi_version", "igpu_last_error_string", "igpu_plan_create", "igpu_plan_destroy", "igpu_plan_query",
     "igpu_bra_pairs", "igpu_atoms", "igpu_schwarz", "igpu_set_mixed_cutoff", "igpu_eri_dense",
-    "igpu_eri_builder_fill", "igpu_density_shell_bounds", "igpu_jk", "igpu_jk_device", "igpu_grad",
+    "igpu_eri_builder_fill", "igpu_density_shell_bounds", "igpu_jk", "igpu_jk_device", "igpu_jk_device_static",
+    "igpu_grad",
     "igpu_grad_device", "igpu_last_stats", "igpu_last_profile",
 ]
 

@@ -26,6 +26,7 @@
 #include "../../include/integral_gpu.h"
 #include "host_math.hpp"
 #include "launch.hpp"
+#include "noalloc.hpp"
 
 using namespace igpu;
 
@@ -858,6 +859,75 @@ int igpu_jk(igpu_plan* P, const double* dens, int ndens, const uint32_t* bra_sub
   for (size_t e = 0; e < n2; ++e) J[e] += tj[e];
   if (want_k)
     for (size_t e = 0; e < n2; ++e) K[e] += tk[e];
+  return IGPU_OK;
+}
+
+int igpu_jk_device_static(igpu_plan* P, const double* d_dens, int ndens, double threshold, int want_k,
+                          double* d_J, double* d_K, void* stream) {
+  if (!P || !d_dens || !d_J) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (ndens < 1 || ndens > MAX_DENS) return fail(IGPU_ERR_DENSITY_COUNT, "1..64 densities");
+  if (want_k && !d_K) return fail(IGPU_ERR_INVALID_ARGUMENT, "exchange buffer required");
+  if (std::isnan(threshold)) return fail(IGPU_ERR_INVALID_ARGUMENT, "threshold is NaN");
+  // the FP64 task list of this threshold must already exist (igpu_jk /
+  // igpu_jk_device with the same threshold build and cache it)
+  auto it = P->jk_tasks.find(std::make_pair(threshold, 0.0));
+  if (it == P->jk_tasks.end())
+    return fail(IGPU_ERR_INVALID_ARGUMENT,
+                "no FP64 task list for this threshold: call igpu_jk or igpu_jk_device with it once first");
+  StaticBufs sb;
+  CK(static_buffers(&sb));
+  const size_t nb = (size_t)ndens * P->nsh * P->nsh;
+  if (nb > sb.bounds_doubles)
+    return fail(IGPU_ERR_UNSUPPORTED, "ndens * nsh^2 exceeds the static bounds storage (" +
+                                          std::to_string(sb.bounds_doubles) + " doubles)");
+  TaskSet& ts = *it->second;
+  const size_t nl = ts.launches.size();
+  if (nl > (size_t)sb.max_launches) return fail(IGPU_ERR_UNSUPPORTED, "too many class launches for static storage");
+  for (auto& L : ts.launches) {
+    if (L->total == 0) continue;
+    const KernelEntry* e = kernel_entry(L->pcb, L->pck);
+    if (!e) return fail(IGPU_ERR_UNSUPPORTED, "angular class not compiled for the GPU");
+    if ((size_t)(128 / e->team) * e->slot > sb.scratch_doubles)
+      return fail(IGPU_ERR_UNSUPPORTED, "class scratch exceeds the static scratch storage");
+  }
+  cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
+  CK(launch_shell_block_max(d_dens, ndens, P->d_shells.p, P->nsh, P->nao, 0, sb.bounds, s));
+  // the work counters must start at zero; the scratch slots are written
+  // before they are read (general image path: no running accumulators)
+  CK(cudaMemsetAsync(sb.work, 0, nl * sizeof(unsigned long long), s));
+  KernelArgs A = base_args(P);
+  A.mode = MODE_JK;
+  A.counters = nullptr;
+  A.jk.D = d_dens;
+  A.jk.bounds = sb.bounds;
+  A.jk.ndens = ndens;
+  A.jk.want_k = want_k ? 1 : 0;
+  A.jk.symmetric = 0;
+  A.jk.threshold = threshold;
+  A.jk.J = d_J;
+  A.jk.K = want_k ? d_K : nullptr;
+  A.scratch = sb.scratch;
+  for (size_t li = 0; li < nl; ++li) {
+    Launch* L = ts.launches[li].get();
+    if (L->total == 0) continue;
+    const KernelEntry* e = kernel_entry(L->pcb, L->pck);
+    const size_t teams = 128 / e->team;
+    const size_t cap = sb.scratch_doubles / (teams * e->slot);
+    const size_t grid = std::min(grid_for(e, false, L->total), cap);
+    A.slot_doubles = e->slot;
+    A.acc_offset = e->slot;
+    A.work_counter = sb.work + li;
+    A.chunk = (unsigned long long)(32 / e->team) * 16;
+    A.task.bra_pair = L->bra_pair.p;
+    A.task.ket_pairs = L->ket_list;
+    A.task.prefix = L->prefix.p;
+    A.task.ket_start = L->ket_start.n ? L->ket_start.p : nullptr;
+    A.task.nbra = L->nbra;
+    A.task.total = L->total;
+    A.fp32 = 0;
+    A.builder_swap = 0;
+    CK(launch_quartets(e, false, (int)grid, A, s));
+  }
   return IGPU_OK;
 }
 
