@@ -156,20 +156,22 @@ int igpu_jk_device(igpu_plan* plan, const double* d_dens, int ndens, const uint3
                    size_t nsub, double threshold, int want_k, int precision, double* d_J,
                    double* d_K, void* stream);
 
-/* Allocation-free variant of igpu_jk_device (no counterpart in the
- * reference; added for callers that capture the build in a CUDA graph or
- * must not allocate): FP64, every canonical bra pair, J += and K +=
- * directly (any density, symmetric or not).  Its team scratch (64 MiB),
- * density bounds (ndens * nsh^2 <= 2^21 doubles) and work counters live in
- * file-scope device storage whose addresses are resolved once per device;
- * the call makes no cudaMalloc/cudaFree, no host synchronisation and only
- * memset + kernel launches on `stream`.  Preconditions: the FP64 task list
- * of `threshold` exists (one earlier igpu_jk or igpu_jk_device call on this
- * plan with the same threshold), and the first igpu_jk_device_static call
- * on each device happens outside stream capture.  Oversize requests return
- * IGPU_ERR_UNSUPPORTED.  The storage is shared by every plan on the device:
- * calls must be ordered (one stream), never concurrent.  Does not update
- * igpu_last_stats / igpu_last_profile. */
+/* igpu_jk_device without any device allocation.  It has no counterpart in
+ * the reference.  It is for callers that may not call cudaMalloc/cudaFree
+ * while they run: an SCF driver whose device memory is all handed out by
+ * its own pool allocator, or a pipeline in which cudaFree's implicit device
+ * synchronisation would stall other streams.  FP64, every canonical bra
+ * pair, J += and K += directly (any density, symmetric or not).
+ * Its scratch lives in file-scope device arrays that every GPU loading this
+ * library holds until the process exits: team scratch 64 MiB, density
+ * bounds ndens * nsh^2 <= 2^21 doubles, 1024 work counters.  A request
+ * beyond those sizes returns IGPU_ERR_UNSUPPORTED with a message.  The
+ * first call on a device looks up the arrays' device addresses (set-up);
+ * make that first call before any stream capture.  Every call shares the
+ * arrays, so calls that overlap on the GPU race: order them on one stream.
+ * Also needs the FP64 task list of `threshold`, built by one earlier
+ * igpu_jk or igpu_jk_device call on this plan with the same threshold.
+ * Does not update igpu_last_stats / igpu_last_profile. */
 int igpu_jk_device_static(igpu_plan* plan, const double* d_dens, int ndens, double threshold, int want_k,
                           double* d_J, double* d_K, void* stream);
 

@@ -1,5 +1,7 @@
-"""The allocation-free J/K entry point (igpu_jk_device_static) against the
-allocating one (igpu_jk_device) on the same device-resident densities.
+"""The J/K entry point that allocates no device memory
+(igpu_jk_device_static, for callers whose device memory is owned by their
+own pool allocator) against the allocating one (igpu_jk_device) on the same
+device-resident densities, within the J/K tolerance of the other GPU tests.
 
 Collected last on purpose (file name): it must pass after every other GPU
 test has run in the same process, and alone.
