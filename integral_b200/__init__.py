@@ -392,10 +392,17 @@ class DirectContractor:
             float(threshold), int(bool(want_exchange)), int(precision), ctypes.c_void_p(d_J),
             ctypes.c_void_p(d_K if want_exchange else 0), ctypes.c_void_p(stream or 0)))
 
+    def set_mixed_cutoff(self, cutoff: float):
+        """MIXED precision: quartets with Q_bra*Q_ket*max|D| below `cutoff`
+        (default 1e-4) run in FP32 (igpu_set_mixed_cutoff)."""
+        _lib.check(_lib.lib().igpu_set_mixed_cutoff(self._plan.h, float(cutoff)))
+
     def jk_device_static(self, d_dens, ndens, d_J, d_K, threshold, want_exchange=True, stream=None):
-        """Allocation-free FP64 J/K on device pointers (igpu_jk_device_static):
-        needs one earlier jk/jk_device call with the same threshold; adds into
-        J and K without synchronising the stream."""
+        """FP64 J/K on device pointers that allocates no device memory
+        (igpu_jk_device_static), for callers whose device memory belongs to
+        their own pool allocator or that cannot afford cudaFree's implicit
+        synchronisation.  Needs one earlier jk/jk_device call with the same
+        threshold; adds into J and K; calls sharing a GPU must not overlap."""
         _lib.check(_lib.lib().igpu_jk_device_static(
             self._plan.h, ctypes.c_void_p(d_dens), ndens, float(threshold), int(bool(want_exchange)),
             ctypes.c_void_p(d_J), ctypes.c_void_p(d_K if want_exchange else 0), ctypes.c_void_p(stream or 0)))

@@ -24,8 +24,8 @@ void register_one(KernelEntry* tab, int npc) {
   e.k64 = quartet_kernel<LA, LB, LC, LD, double>;
   e.k32 = quartet_kernel<LA, LB, LC, LD, float>;
   e.team = TeamShape<LA, LB, LC, LD, double>::T;
-  e.smem64 = (128 / e.team) * TeamShape<LA, LB, LC, LD, double>::SMEM_PER_TEAM * (int)sizeof(double);
-  e.smem32 = (128 / e.team) * TeamShape<LA, LB, LC, LD, float>::SMEM_PER_TEAM * (int)sizeof(float);
+  e.smem64 = (128 / e.team) * TeamShape<LA, LB, LC, LD, double>::TEAM_BYTES;
+  e.smem32 = (128 / e.team) * TeamShape<LA, LB, LC, LD, float>::TEAM_BYTES;
   e.slot = slot_layout(LA, LB, LC, LD).total;
   e.valid = true;
   tab[PCB * npc + PCK] = e;

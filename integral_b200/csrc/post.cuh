@@ -410,37 +410,111 @@ __device__ __forceinline__ void flush_bra_acc(const KernelArgs& A, double* acc, 
   __syncwarp(tmask);
 }
 
+// Symmetric densities: one orientation of every image, the six
+// contractions
+//   t0 J'[A a][B b] += w0 sum_cd B D[C c][D d]   (running bra accumulator)
+//   t1 J'[C c][D d] += w1 sum_ab B D[A a][B b]
+//   t2 K'[A a][C c] += w2 sum_bd B D[B b][D d]   t3 K'[B b][C c] += w3 sum_ad B D[A a][D d]
+//   t4 K'[A a][D d] += w4 sum_bc B D[B b][C c]   t5 K'[B b][D d] += w5 sum_ac B D[A a][C c]
+// with the summed weights of the permutation images landing on each block
+// or its transpose.  All output elements of all six terms form one list
+// spread over the team's lanes; each lane sums its elements for up to DCH
+// densities at once (densities d0 + k with bit k of m set), so every block
+// element read feeds up to DCH products.
+constexpr int JK_DCH = 4;
+
+template <int DCH>
+__device__ __forceinline__ void jk_sym_chunk(const KernelArgs& A, const double* B, const int dims[4],
+                                             const int offs[4], const double wt[6], int nterm, int d0, unsigned m,
+                                             double* acc, int lane, int T) {
+  // (u, v) output axes and (s, t) summed axes of term t, one nibble per term
+  // (no dynamically indexed local arrays); D block rows on s, columns on t
+  constexpr unsigned PU = 0x101020u, PV = 0x332231u, PS = 0x010102u, PT = 0x223313u;
+  const int st0 = dims[1] * dims[2] * dims[3], st1 = dims[2] * dims[3], st2 = dims[3];
+  auto stride = [&](int ax) { return ax == 0 ? st0 : (ax == 1 ? st1 : (ax == 2 ? st2 : 1)); };
+  auto dim = [&](int ax) { return ax == 0 ? dims[0] : (ax == 1 ? dims[1] : (ax == 2 ? dims[2] : dims[3])); };
+  auto off = [&](int ax) { return ax == 0 ? offs[0] : (ax == 1 ? offs[1] : (ax == 2 ? offs[2] : offs[3])); };
+  auto nib = [](unsigned p, int t) { return (int)((p >> (4 * t)) & 0xFu); };
+  const int nab = dims[0] * dims[1];
+  const int nao = A.nao;
+  const size_t n2 = (size_t)nao * nao;
+  auto len = [&](int t) { return (t < nterm && wt[t] != 0.0) ? dim(nib(PU, t)) * dim(nib(PV, t)) : 0; };
+  const int e1 = len(0), e2 = e1 + len(1), e3 = e2 + len(2), e4 = e3 + len(3), e5 = e4 + len(4), e6 = e5 + len(5);
+  for (int q = lane; q < e6; q += T) {
+    const int t = q < e1 ? 0 : (q < e2 ? 1 : (q < e3 ? 2 : (q < e4 ? 3 : (q < e5 ? 4 : 5))));
+    const int base = t == 0 ? 0 : (t == 1 ? e1 : (t == 2 ? e2 : (t == 3 ? e3 : (t == 4 ? e4 : e5))));
+    const double w = t == 0 ? wt[0] : (t == 1 ? wt[1] : (t == 2 ? wt[2] : (t == 3 ? wt[3] : (t == 4 ? wt[4] : wt[5]))));
+    const int u = nib(PU, t), v = nib(PV, t), s = nib(PS, t), tt = nib(PT, t);
+    const int r = q - base;
+    const int nv = dim(v);
+    const int iu = r / nv, iv = r - iu * nv;
+    const int ns = dim(s), nt = dim(tt);
+    const double* Bp = B + (size_t)iu * stride(u) + (size_t)iv * stride(v);
+    const int ss = stride(s), stt = stride(tt);
+    const double* Dp = A.jk.D + (size_t)d0 * n2 + (size_t)off(s) * nao + off(tt);
+    double sum[DCH];
+#pragma unroll
+    for (int k = 0; k < DCH; ++k) sum[k] = 0.0;
+    for (int is = 0; is < ns; ++is) {
+      const double* br = Bp + (size_t)is * ss;
+      const double* dr = Dp + (size_t)is * nao;
+      for (int it = 0; it < nt; ++it) {
+        const double b = br[(size_t)it * stt];
+#pragma unroll
+        for (int k = 0; k < DCH; ++k)
+          if ((m >> k) & 1u) sum[k] += b * __ldg(dr + (size_t)k * n2 + it);
+      }
+    }
+    if (t == 0) {
+#pragma unroll
+      for (int k = 0; k < DCH; ++k)
+        if ((m >> k) & 1u) acc[1 + (size_t)(d0 + k) * nab + r] += w * sum[k];
+    } else {
+      double* out = t == 1 ? A.jk.J : A.jk.K;
+      const size_t o = (size_t)(off(u) + iu) * nao + off(v) + iv;
+#pragma unroll
+      for (int k = 0; k < DCH; ++k)
+        if ((m >> k) & 1u) atomicAdd(out + (size_t)(d0 + k) * n2 + o, w * sum[k]);
+    }
+  }
+}
+
+// Shared memory a team needs for its copy of the Cartesian block la..ld.
+__host__ __device__ constexpr int jk_stage_doubles(int la, int lb, int lc, int ld) {
+  return ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+}
+
 __device__ __forceinline__ void consume_jk(const KernelArgs& A, const double* B, const int dims[4],
                                            const int offs[4], const int sh[4], uint64_t mask, int lane, int T,
-                                           double* acc, int pbi, unsigned tmask) {
+                                           double* acc, int pbi, unsigned tmask, double* stage) {
   const unsigned w = distinct_perms(sh);
   auto W = [&](int p) { return (double)((w >> p) & 1u); };
   const int nao = A.nao;
   const size_t n2 = (size_t)nao * nao;
   if (A.jk.symmetric) {
-    // One orientation of every image: J'[A a][B b], J'[C c][D d], K'[A a][C c],
-    // K'[B b][C c], K'[A a][D d], K'[B b][D d] with the summed weights of the
-    // permutations landing on the block or its transpose.
     if ((int)acc[0] != pbi) {
       flush_bra_acc(A, acc, lane, T, tmask);
       if (lane == 0) acc[0] = (double)pbi;
       __syncwarp(tmask);
     }
-    const int nab = dims[0] * dims[1];
-    for (int d = 0; d < A.jk.ndens; ++d) {
-      if (!((mask >> d) & 1ull)) continue;
-      const double* Dm = A.jk.D + d * n2;
-      double* J = A.jk.J + d * n2;
-      double* K = A.jk.want_k ? A.jk.K + d * n2 : nullptr;
-      jk_term_acc(B, dims, offs, nao, Dm, W(0) + W(1) + W(2) + W(3), acc + 1 + (size_t)d * nab, lane, T);
-      jk_term(B, dims, offs, nao, 2, 3, 0, 1, Dm, 0, 1, J, W(4) + W(5) + W(6) + W(7), J, 0.0, lane, T);
-      if (K) {
-        jk_term(B, dims, offs, nao, 0, 2, 1, 3, Dm, 1, 3, K, W(0) + W(4), K, 0.0, lane, T);
-        jk_term(B, dims, offs, nao, 1, 2, 0, 3, Dm, 0, 3, K, W(1) + W(5), K, 0.0, lane, T);
-        jk_term(B, dims, offs, nao, 0, 3, 1, 2, Dm, 1, 2, K, W(2) + W(6), K, 0.0, lane, T);
-        jk_term(B, dims, offs, nao, 1, 3, 0, 2, Dm, 0, 2, K, W(3) + W(7), K, 0.0, lane, T);
-      }
+    const double wt[6] = {W(0) + W(1) + W(2) + W(3), W(4) + W(5) + W(6) + W(7), W(0) + W(4),
+                          W(1) + W(5),               W(2) + W(6),               W(3) + W(7)};
+    const int nterm = A.jk.want_k ? 6 : 2;
+    // the sums read the block with lane-dependent strides: work from a
+    // shared-memory copy (one coalesced pass) when the team has one
+    const double* Bs = B;
+    if (stage) {
+      const int nblk = dims[0] * dims[1] * dims[2] * dims[3];
+      for (int q = lane; q < nblk; q += T) stage[q] = B[q];
+      __syncwarp(tmask);
+      Bs = stage;
     }
+    const unsigned long long live = A.jk.ndens >= 64 ? ~0ull : ((1ull << A.jk.ndens) - 1ull);
+    for (int d0 = 0; d0 < A.jk.ndens; d0 += JK_DCH) {
+      const unsigned m = (unsigned)(((mask & live) >> d0) & ((1u << JK_DCH) - 1u));
+      if (m) jk_sym_chunk<JK_DCH>(A, Bs, dims, offs, wt, nterm, d0, m, acc, lane, T);
+    }
+    __syncwarp(tmask);
     return;
   }
   for (int d = 0; d < A.jk.ndens; ++d) {
@@ -544,7 +618,7 @@ __device__ __forceinline__ void consume_schwarz(const KernelArgs& A, const doubl
 // block -> consumer.
 __device__ __forceinline__ void post_quartet(const KernelArgs& A, const ClassDims& cd_, const PairD& pb,
                                              const PairD& pk, const Screen& sc, double* slot, int lane, int T,
-                                             unsigned tmask, int pb_index) {
+                                             unsigned tmask, int pb_index, double* stage) {
   const int la = cd_.la, lb = cd_.lb, lc = cd_.lc, ld = cd_.ld;
   const SlotLayout L = slot_layout(la, lb, lc, ld);
   double* buf[3] = {slot, slot + L.S, slot + 2 * L.S};
@@ -565,7 +639,7 @@ __device__ __forceinline__ void post_quartet(const KernelArgs& A, const ClassDim
   const int offs[4] = {s0.off, s1.off, s2.off, s3.off};
   switch (A.mode) {
     case MODE_JK:
-      consume_jk(A, B, dims, offs, shl, sc.mask, lane, T, slot + A.acc_offset, pb_index, tmask);
+      consume_jk(A, B, dims, offs, shl, sc.mask, lane, T, slot + A.acc_offset, pb_index, tmask, stage);
       break;
     case MODE_DENSE:
       consume_dense(A, B, dims, offs, shl, lane, T);
@@ -579,6 +653,103 @@ __device__ __forceinline__ void post_quartet(const KernelArgs& A, const ClassDim
     default:
       break;
   }
+}
+
+// ----------------------------------------- J/K post phase, Cartesian classes
+
+// One contraction term of the symmetric J/K images with the block shape
+// known at compile time: output (u, v), summed (s, t), D block rows on s and
+// columns on t.  Every sum is fully unrolled, so its block and density loads
+// are independent and in flight together.
+template <int U, int V, int S, int TT, int N0, int N1, int N2, int N3, int T, bool ACC>
+__device__ __forceinline__ void jk_term_ct(const KernelArgs& A, const double* B, const int offs[4], double w, int d0,
+                                           unsigned m, double* out, int lane) {
+  constexpr int N[4] = {N0, N1, N2, N3};
+  constexpr int ST[4] = {N1 * N2 * N3, N2 * N3, N3, 1};
+  constexpr int NU = N[U], NV = N[V], NS = N[S], NT = N[TT];
+  constexpr int DCH = JK_DCH;
+  const int nao = A.nao;
+  const size_t n2 = (size_t)nao * nao;
+  const double* Dp = A.jk.D + (size_t)d0 * n2 + (size_t)offs[S] * nao + offs[TT];
+  for (int r = lane; r < NU * NV; r += T) {
+    const int iu = r / NV, iv = r - (r / NV) * NV;
+    const double* Bp = B + iu * ST[U] + iv * ST[V];
+    double sum[DCH];
+#pragma unroll
+    for (int k = 0; k < DCH; ++k) sum[k] = 0.0;
+#pragma unroll
+    for (int is = 0; is < NS; ++is)
+#pragma unroll
+      for (int it = 0; it < NT; ++it) {
+        const double b = Bp[is * ST[S] + it * ST[TT]];
+#pragma unroll
+        for (int k = 0; k < DCH; ++k)
+          if ((m >> k) & 1u) sum[k] += b * __ldg(Dp + k * n2 + (size_t)is * nao + it);
+      }
+    if (ACC) {
+#pragma unroll
+      for (int k = 0; k < DCH; ++k)
+        if ((m >> k) & 1u) out[1 + (size_t)(d0 + k) * (N0 * N1) + r] += w * sum[k];
+    } else {
+      const size_t o = (size_t)(offs[U] + iu) * nao + offs[V] + iv;
+#pragma unroll
+      for (int k = 0; k < DCH; ++k)
+        if ((m >> k) & 1u) atomicAdd(out + (size_t)(d0 + k) * n2 + o, w * sum[k]);
+    }
+  }
+}
+
+// Post phase of a symmetric J/K quartet whose four shells are Cartesian:
+// horizontal recurrences into the slot, the block copied to the team's
+// shared memory (when it has room), then the six image contractions of
+// consume_jk with the shape fixed at compile time.
+template <int LA, int LB, int LC, int LD, int T>
+__device__ __forceinline__ void post_quartet_jk_cart(const KernelArgs& A, const PairD& pb, const PairD& pk,
+                                                     const Screen& sc, double* slot, int lane, unsigned tmask, int pbi,
+                                                     double* stage) {
+  constexpr int N0 = ncart(LA), N1 = ncart(LB), N2 = ncart(LC), N3 = ncart(LD);
+  constexpr int NBLK = N0 * N1 * N2 * N3;
+  const SlotLayout L = slot_layout(LA, LB, LC, LD);
+  double* buf[3] = {slot, slot + L.S, slot + 2 * L.S};
+  double* blk = slot + 3 * L.S;
+  const double ab[3] = {pb.abx, pb.aby, pb.abz};
+  const double cdv[3] = {pk.abx, pk.aby, pk.abz};
+  int cur = 0;
+  hrr_bra(buf, cur, LA, LB, nrange(LC, LC + LD), ab, lane, T, tmask);
+  hrr_ket(buf, cur, blk, LA, LB, LC, LD, nrange(LC, LC + LD), cdv, lane, T, tmask);
+  const double* B = blk;
+  if (stage) {
+    for (int q = lane; q < NBLK; q += T) stage[q] = blk[q];
+    __syncwarp(tmask);
+    B = stage;
+  }
+  const int shl[4] = {pb.a, pb.b, pk.a, pk.b};
+  const int offs[4] = {A.shells[shl[0]].off, A.shells[shl[1]].off, A.shells[shl[2]].off, A.shells[shl[3]].off};
+  double* acc = slot + A.acc_offset;
+  if ((int)acc[0] != pbi) {
+    flush_bra_acc(A, acc, lane, T, tmask);
+    if (lane == 0) acc[0] = (double)pbi;
+    __syncwarp(tmask);
+  }
+  const unsigned wp = distinct_perms(shl);
+  auto W = [&](int p) { return (double)((wp >> p) & 1u); };
+  const double w0 = W(0) + W(1) + W(2) + W(3), w1 = W(4) + W(5) + W(6) + W(7);
+  const double w2 = W(0) + W(4), w3 = W(1) + W(5), w4 = W(2) + W(6), w5 = W(3) + W(7);
+  const unsigned long long live = A.jk.ndens >= 64 ? ~0ull : ((1ull << A.jk.ndens) - 1ull);
+  const uint64_t mask = sc.mask & live;
+  for (int d0 = 0; d0 < A.jk.ndens; d0 += JK_DCH) {
+    const unsigned m = (unsigned)((mask >> d0) & ((1u << JK_DCH) - 1u));
+    if (!m) continue;
+    jk_term_ct<0, 1, 2, 3, N0, N1, N2, N3, T, true>(A, B, offs, w0, d0, m, acc, lane);
+    if (w1 != 0.0) jk_term_ct<2, 3, 0, 1, N0, N1, N2, N3, T, false>(A, B, offs, w1, d0, m, A.jk.J, lane);
+    if (A.jk.want_k) {
+      if (w2 != 0.0) jk_term_ct<0, 2, 1, 3, N0, N1, N2, N3, T, false>(A, B, offs, w2, d0, m, A.jk.K, lane);
+      if (w3 != 0.0) jk_term_ct<1, 2, 0, 3, N0, N1, N2, N3, T, false>(A, B, offs, w3, d0, m, A.jk.K, lane);
+      if (w4 != 0.0) jk_term_ct<0, 3, 1, 2, N0, N1, N2, N3, T, false>(A, B, offs, w4, d0, m, A.jk.K, lane);
+      if (w5 != 0.0) jk_term_ct<1, 3, 0, 2, N0, N1, N2, N3, T, false>(A, B, offs, w5, d0, m, A.jk.K, lane);
+    }
+  }
+  __syncwarp(tmask);
 }
 
 }  // namespace igpu

@@ -73,6 +73,15 @@ struct TeamShape {
   static constexpr int BP = BP0 >= T ? T : (BP0 >= 16 ? 16 : (BP0 >= 8 ? 8 : (BP0 >= 4 ? 4 : (BP0 >= 2 ? 2 : 1))));
   static constexpr int SUB = T / BP;  // lanes sharing one primitive quartet in a round
   static constexpr int SMEM_PER_TEAM = T == 1 ? 0 : BP * PRIM_TAB;  // in R units
+  // Per-team shared memory: the primitive tables of phase 1, reused by the
+  // post phase for the team's copy of the Cartesian block (16-byte multiple).
+  // Classes whose copies would need more than 96 KB per 128-thread block
+  // (f shells) read the block from the scratch slot instead.
+  static constexpr int STAGE_BYTES0 = T == 1 ? 0 : jk_stage_doubles(LA, LB, LC, LD) * 8;
+  static constexpr bool STAGE = T > 1 && (128 / T) * STAGE_BYTES0 <= 96 * 1024;
+  static constexpr int STAGE_BYTES = STAGE ? STAGE_BYTES0 : 0;
+  static constexpr int TAB_BYTES = SMEM_PER_TEAM * (int)sizeof(R);
+  static constexpr int TEAM_BYTES = ((TAB_BYTES > STAGE_BYTES ? TAB_BYTES : STAGE_BYTES) + 15) / 16 * 16;
 };
 
 // ------------------------------------------------------------- TEAM == 1
@@ -271,8 +280,20 @@ __device__ __forceinline__ void team_chunks(const KernelArgs& A, const R* s_tab,
 
 // ------------------------------------------------------------------ kernel
 
+// Minimum resident 128-thread blocks per SM (register budget): team
+// classes 3 (168 registers; measured faster than the unconstrained
+// allocation, whose unrolled J/K sums take up to 255), thread-per-quartet
+// classes by the size of their register-resident G table (spilling large
+// tables costs more than the occupancy gains).
+template <int LA, int LB, int LC, int LD>
+__host__ __device__ constexpr int quartet_min_blocks() {
+  return team_size<LA, LB, LC, LD>() > 1
+             ? 3
+             : (ClassShape<LA, LB, LC, LD>::NG <= 9 ? 5 : (ClassShape<LA, LB, LC, LD>::NG <= 27 ? 3 : 1));
+}
+
 template <int LA, int LB, int LC, int LD, typename R>
-__global__ void __launch_bounds__(128) quartet_kernel(KernelArgs A) {
+__global__ void __launch_bounds__(128, quartet_min_blocks<LA, LB, LC, LD>()) quartet_kernel(KernelArgs A) {
   using S = ClassShape<LA, LB, LC, LD>;
   using TS = TeamShape<LA, LB, LC, LD, R>;
   constexpr int T = TS::T;
@@ -284,7 +305,9 @@ __global__ void __launch_bounds__(128) quartet_kernel(KernelArgs A) {
   const int lane = threadIdx.x % T;
   const int nteams = (gridDim.x * blockDim.x) / T;
   const unsigned tmask = T == 32 ? 0xffffffffu : (((1u << T) - 1u) << ((threadIdx.x % 32) / T * T));
-  R* sm = reinterpret_cast<R*>(smem_raw) + (size_t)(threadIdx.x / T) * TS::SMEM_PER_TEAM;
+  unsigned char* team_smem = smem_raw + (size_t)(threadIdx.x / T) * TS::TEAM_BYTES;
+  R* sm = reinterpret_cast<R*>(team_smem);
+  double* stage = TS::STAGE ? reinterpret_cast<double*>(team_smem) : nullptr;
   double* slot = A.scratch + (size_t)team * A.slot_doubles;
   QuartetCounters cnt;
   const ClassDims dims{LA, LB, LC, LD};
@@ -338,7 +361,13 @@ __global__ void __launch_bounds__(128) quartet_kernel(KernelArgs A) {
         team_chunks<LA, LB, LC, LD, R, 0>(A, s_tab, pb, pk, sm, lane, tmask, slot);
       }
       __syncwarp(tmask);
-      post_quartet(A, dims, pb, pk, sc, slot, lane, T, tmask, pbi);
+      if constexpr (T > 1) {
+        if (use_acc && A.kinds == 0) {
+          post_quartet_jk_cart<LA, LB, LC, LD, T>(A, pb, pk, sc, slot, lane, tmask, pbi, stage);
+          continue;
+        }
+      }
+      post_quartet(A, dims, pb, pk, sc, slot, lane, T, tmask, pbi, stage);
       __syncwarp(tmask);
     }
   }

@@ -168,6 +168,20 @@ def test_jk_full_size_quartet_list_and_sampled_parity():
     assert float(np.max(np.abs(K - Ko))) < 1e-12 * float(np.max(np.abs(Ko)))
 
 
+def test_jk_spherical_f_shells_matches_oracle():
+    """The 200-atom spherical recipe (s,s,s,p,p,d,d,f; 4 primitives
+    0.08*2.2^k; tau 1e-11) on 4 atoms: every class up to (ff|ff) in real
+    solid harmonics, exact quartet list and J/K within 1e-12."""
+    s = S.jk_spherical_system(natom=4, side=6.0, ndens=2, nocc=40)
+    dc = ib.Basis(s["shells"]).direct_contractor()
+    J, K = dc.jk(s["dens"], s["threshold"])
+    st = dc.last_stats()
+    Jo, Ko, cnt, hsh = O.OracleBasis(s["shells"]).direct_jk(s["dens"], s["threshold"], nthreads=os.cpu_count() or 8)
+    assert st["quartets"] == cnt and st["quartet_hash"] == hsh
+    assert float(np.max(np.abs(J - Jo))) < 1e-12 * float(np.max(np.abs(Jo)))
+    assert float(np.max(np.abs(K - Ko))) < 1e-12 * float(np.max(np.abs(Ko)))
+
+
 def test_mixed_precision_energy_error_full_size():
     s = S.jk_system()
     dc = ib.Basis(s["shells"]).direct_contractor()
