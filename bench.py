@@ -44,6 +44,11 @@ sys.path.insert(0, ROOT)
 METRIC = "Fock J/K build quartets/s (FP32-mixed, <=1e-6 Eh vs FP64) on B200"
 UNIT = "quartets/s"
 
+# dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch of
+# this workload's kernels, from a one-pass ncu capture on a B200
+# (profiles/quartet_kernel_2120_fp32_traffic.md); bytes per launch.
+NCU_TRAFFIC = {"quartet_kernel(21|20) fp32": 612.62e6 + 526.42e6}
+
 
 def parse():
     p = argparse.ArgumentParser()
@@ -52,7 +57,97 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-sample-bras", type=int, default=24)
+    p.add_argument("--workload", default="jk", choices=["jk", "grad"],
+                   help="jk: the headline J/K build (default); grad: the density-direct ERI gradient of the "
+                        "100-atom / nao 1400 system on an interleaved 1/--grad-stride share of the bra pairs")
+    # a stride > 1 still decodes every task (the subset is a filter), so its
+    # quartets/s understates the full build's
+    p.add_argument("--grad-stride", type=int, default=1)
+    p.add_argument("--profile-case", action="store_true",
+                   help="one FP32-mixed J/K build of the 24-atom (nao 360) system and its per-launch "
+                        "records, no timing: the small case for ncu captures")
     return p.parse_args()
+
+
+def grad_bench(args):
+    """Density-direct ERI gradient (DirectGradContractor) of the 100-atom,
+    nao 1400 Cartesian s,s,p,p,d system with Coulomb (1/2, D, D) and exchange
+    (-1/4, D, D) terms at tau 1e-12, over every --grad-stride-th canonical bra
+    pair (gradient contributions are additive per bra pair).  FP32-mixed is
+    the value, FP64 beside it; device time of the C-ABI call (term matrices
+    resident after the first call's upload is not separated: host buffers in,
+    natom x 3 out)."""
+    import torch
+
+    torch.cuda.set_device(0)
+    import integral_b200 as ib
+    from integral_b200 import systems as S
+
+    s = S.grad_system()
+    gc = ib.Basis(s["shells"]).direct_grad_contractor()
+    dens = gc.density([ib.GradDensityTerm(f, l, r) for f, l, r in s["coulomb"]],
+                      [ib.GradDensityTerm(f, l, r) for f, l, r in s["exchange"]])
+    bras = np.arange(0, len(gc.bra_pairs()), args.grad_stride)
+
+    def run(prec):
+        out = np.zeros((gc.natom(), 3))
+        t = time.time()
+        gc.accumulate_bra_pairs(ib.DirectGradWorkspace(), bras, dens, s["threshold"], out, prec)
+        wall = time.time() - t
+        st = gc.last_stats()
+        return out, st, wall
+
+    res = {}
+    for prec in (1, 0):
+        for _ in range(args.warmup):
+            run(prec)
+        ms, q, flops, wall = 0.0, 0, 0.0, 0.0
+        for _ in range(args.steps):
+            out, st, w = run(prec)
+            ms += st["kernel_ms"]
+            q += st["quartets"]
+            flops += st["model_flops"]
+            wall += w
+        res[prec] = (out, ms, q, flops, wall)
+    g32, ms32, q32, f32, w32 = res[1]
+    g64, ms64, q64, f64, w64 = res[0]
+    line = {
+        "metric": "density-direct ERI gradient quartets/s (FP32-mixed) on B200", "unit": "quartets/s",
+        "value": q32 / (ms32 * 1e-3), "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "fp32-mixed (fp64 accumulation)", "data": "synthetic (seeded generator, no data set)",
+        "config": {"workload": "ERI gradient, 100 atoms in 24-bohr cube, s,s,p,p,d Cartesian, nao 1400, "
+                               "Coulomb (1/2,D,D) + exchange (-1/4,D,D), tau 1e-12, every %d-th bra pair"
+                               % args.grad_stride, "quartets_per_step": q32 // args.steps},
+        "fp64": {"value": q64 / (ms64 * 1e-3), "unit": "quartets/s", "ms_per_step": ms64 / args.steps,
+                 "model_tflops": f64 / (ms64 * 1e-3) / 1e12},
+        "model_tflops": f32 / (ms32 * 1e-3) / 1e12,
+        "max_abs_mixed_minus_fp64": float(np.abs(g32 - g64).max()),
+        "max_abs_gradient": float(np.abs(g64).max()),
+        "e2e": {"value": q32 / w32, "unit": "quartets/s"},
+    }
+    print(json.dumps(line))
+
+
+def profile_case():
+    """One mixed J/K build of a 24-atom cut of the bench recipe (12-bohr
+    cube): every class of the bench, inputs larger than L2 are not needed
+    because the kernels are compute bound; prints the launch records."""
+    import torch
+
+    torch.cuda.set_device(0)
+    import integral_b200 as ib
+    from integral_b200 import systems as S
+
+    s = S.jk_system(natom=24, side=12.0)
+    dc = ib.Basis(s["shells"]).direct_contractor()
+    dc.jk(s["dens"], s["threshold"], precision=1)
+    st = dc.last_stats()
+    print(json.dumps({"case": "direct J/K, 24 atoms, nao %d, 4 densities, mixed" % S.nao_of(s["shells"]),
+                      "quartets": st["quartets"], "quartets_fp32": st["quartets_fp32"],
+                      "kernel_ms": st["kernel_ms"]}))
+    for r in dc.plan.profile():
+        print(json.dumps(r))
 
 
 def dist_env():
@@ -199,6 +294,10 @@ def reference_arm(args):
 
 def main():
     args = parse()
+    if args.profile_case:
+        return profile_case()
+    if args.workload == "grad":
+        return grad_bench(args)
     if args.impl == "reference":
         return reference_arm(args)
     import torch
@@ -375,7 +474,9 @@ def main():
                                     "MEASURED_PEAKS.json)" % ("SGEMM, TF32 off" if top["fp32"] else "DGEMM"),
                      "flops_model": "fixed Rys flop model of the reference algorithm per surviving primitive "
                                     "quartet (+J/K contraction)",
-                     "traffic": None,
+                     "traffic": NCU_TRAFFIC.get("quartet_kernel(%d%d|%d%d) %s" % (
+                         top["la"], top["lb"], top["lc"], top["ld"], "fp32" if top["fp32"] else "fp64")),
+                     "traffic_unit": "bytes per launch (ncu dram read + write, one capture of this workload)",
                      "all_kernels_model_tflops": total_model / (kernel_ms * 1e-3) / 1e12},
         "clocks": clocks,
         "gpu_launches": l_mixed,

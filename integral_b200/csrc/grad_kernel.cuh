@@ -628,6 +628,141 @@ __device__ __forceinline__ void grad_post(const KernelArgs& A, int la, int lb, i
   }
 }
 
+// ------------------------------------------ phase 2, Cartesian classes
+
+__host__ __device__ constexpr int cidx(int lx, int ly, int lz) { return (ly + lz) * (ly + lz + 1) / 2 + lz; }
+
+// Weight block of an all-Cartesian quartet with compile-time dims (same
+// values as grad_weight_block).  The reference-orientation AO index of each
+// element is picked by selects, not by indexing a local array.
+template <int LA, int LB, int LC, int LD, int T>
+__device__ __forceinline__ void grad_weight_block_cart(const KernelArgs& A, const PairD& pb, const PairD& pk,
+                                                       const Screen& sc, double* W, int lane) {
+  constexpr int N0 = ncart(LA), N1 = ncart(LB), N2 = ncart(LC), N3 = ncart(LD);
+  const int o0 = A.shells[pb.a].off, o1 = A.shells[pb.b].off, o2 = A.shells[pk.a].off, o3 = A.shells[pk.b].off;
+  // evaluation position of reference positions 0..3
+  const int bb = sc.swapped ? 2 : 0, kb = sc.swapped ? 0 : 2;
+  const bool bflip = pb.a != pb.i, kflip = pk.a != pk.i;
+  const int e0 = bb == 0 ? (bflip ? 1 : 0) : (kflip ? 3 : 2);  // eval slot of reference i
+  const int e1 = bb == 0 ? (bflip ? 0 : 1) : (kflip ? 2 : 3);  // of j
+  const int e2 = kb == 2 ? (kflip ? 3 : 2) : (bflip ? 1 : 0);  // of k
+  const int e3 = kb == 2 ? (kflip ? 2 : 3) : (bflip ? 0 : 1);  // of l
+  const size_t n = (size_t)A.nao;
+  const GradDev& G = A.grad;
+  const double deg = sc.degeneracy;
+  for (int q = lane; q < N0 * N1 * N2 * N3; q += T) {
+    const int f3 = q % N3, f2 = (q / N3) % N2, f1 = (q / (N3 * N2)) % N1, f0 = q / (N3 * N2 * N1);
+    const size_t x0 = o0 + f0, x1 = o1 + f1, x2 = o2 + f2, x3 = o3 + f3;
+    auto pick = [&](int e) { return e == 0 ? x0 : (e == 1 ? x1 : (e == 2 ? x2 : x3)); };
+    const size_t m0 = pick(e0), m1 = pick(e1), m2 = pick(e2), m3 = pick(e3);
+    double w = 0.0;
+    for (int t = 0; t < G.ncoul; ++t) {
+      const double* Lm = G.cl[t];
+      const double* Rm = G.cr[t];
+      const double fac = 0.5 * deg * __ldg(G.cf + t);
+      w += fac * (__ldg(Lm + m0 * n + m1) * __ldg(Rm + m2 * n + m3) + __ldg(Rm + m0 * n + m1) * __ldg(Lm + m2 * n + m3));
+    }
+    for (int t = 0; t < G.nexch; ++t) {
+      const double* Lm = G.xl[t];
+      const double* Rm = G.xr[t];
+      const double fac = 0.25 * deg * __ldg(G.xf + t);
+      w += fac * (__ldg(Lm + m0 * n + m2) * __ldg(Rm + m1 * n + m3) + __ldg(Lm + m1 * n + m2) * __ldg(Rm + m0 * n + m3) +
+                  __ldg(Lm + m0 * n + m3) * __ldg(Rm + m1 * n + m2) + __ldg(Lm + m1 * n + m3) * __ldg(Rm + m0 * n + m2));
+    }
+    W[q] = w;
+  }
+}
+
+// grad_dot with the shapes fixed at compile time: lanes take the (outer,
+// inner) index pairs around axis POS, the components along POS are unrolled
+// with their shifted indices known at compile time.
+template <int L0, int L1, int L2, int L3, int POS, bool RAISED, int T>
+__device__ __forceinline__ void grad_dot_ct(const double* W, const double* blk, double g[3], int lane) {
+  constexpr int LS[4] = {L0, L1, L2, L3};
+  constexpr int NC[4] = {ncart(L0), ncart(L1), ncart(L2), ncart(L3)};
+  constexpr int LP = LS[POS], NP = NC[POS];
+  constexpr int INNER = (POS < 3 ? NC[3] : 1) * (POS < 2 ? NC[2] : 1) * (POS < 1 ? NC[1] : 1);
+  constexpr int OUTER = (NC[0] * NC[1] * NC[2] * NC[3]) / (NP * INNER);
+  constexpr int NSH = RAISED ? ncart(LP + 1) : (LP > 0 ? ncart(LP - 1) : 1);
+  for (int os = lane; os < OUTER * INNER; os += T) {
+    const int o = os / INNER, s = os - (os / INNER) * INNER;
+    const double* wr = W + (size_t)o * NP * INNER + s;
+    const double* br = blk + (size_t)o * NSH * INNER + s;
+    static_for<NP>([&](auto ai) {
+      constexpr int a = decltype(ai)::value;
+      constexpr int ax = comp_lx(LP, a), ay = comp_ly(LP, a), az = comp_lz(LP, a);
+      const double w = wr[a * INNER];
+      if constexpr (RAISED) {
+        g[0] += w * br[cidx(ax + 1, ay, az) * INNER];
+        g[1] += w * br[cidx(ax, ay + 1, az) * INNER];
+        g[2] += w * br[cidx(ax, ay, az + 1) * INNER];
+      } else {
+        if constexpr (ax > 0) g[0] -= double(ax) * w * br[cidx(ax - 1, ay, az) * INNER];
+        if constexpr (ay > 0) g[1] -= double(ay) * w * br[cidx(ax, ay - 1, az) * INNER];
+        if constexpr (az > 0) g[2] -= double(az) * w * br[cidx(ax, ay, az - 1) * INNER];
+      }
+    });
+  }
+}
+
+template <int L0, int L1, int L2, int L3, int POS, bool RAISED, int T>
+__device__ __forceinline__ void grad_shifted_ct(const double* tabp, int tab_cols, int row_off, int nrows, int col_off,
+                                                const double* W, double* buf[3], double* blk, const double ab[3],
+                                                const double cd[3], double g[3], int lane, unsigned tmask) {
+  constexpr int NCOLS = nrange(L2, L2 + L3);
+  for (int q = lane; q < nrows * NCOLS; q += T) {
+    const int r = q / NCOLS, c = q - (q / NCOLS) * NCOLS;
+    buf[0][q] = tabp[(size_t)(row_off + r) * tab_cols + col_off + c];
+  }
+  __syncwarp(tmask);
+  int cur = 0;
+  hrr_bra(buf, cur, L0, L1, NCOLS, ab, lane, T, tmask);
+  hrr_ket(buf, cur, blk, L0, L1, L2, L3, NCOLS, cd, lane, T, tmask);
+  constexpr int LS[4] = {L0, L1, L2, L3};
+  constexpr int D0 = POS == 0 ? (RAISED ? -1 : 1) : 0, D1 = POS == 1 ? (RAISED ? -1 : 1) : 0;
+  constexpr int D2 = POS == 2 ? (RAISED ? -1 : 1) : 0;
+  // W and the dot use the unshifted shells
+  grad_dot_ct<L0 + D0, L1 + D1, L2 + D2, L3, POS, RAISED, T>(W, blk, g, lane);
+  (void)LS;
+  __syncwarp(tmask);
+}
+
+// Phase 2 of an all-Cartesian quartet (grad_post with compile-time shapes).
+template <int LA, int LB, int LC, int LD, int T>
+__device__ __forceinline__ void grad_post_cart(const KernelArgs& A, const PairD& pb, const PairD& pk, const Screen& sc,
+                                               double* slot, double g[9], int lane, unsigned tmask) {
+  const GradSlot L = grad_slot_layout(LA, LB, LC, LD);
+  double* W = slot + L.ntab;
+  double* buf[3] = {W + 2 * L.W, W + 2 * L.W + L.S, W + 2 * L.W + 2 * L.S};
+  double* blk = W + 2 * L.W + 3 * L.S;
+  grad_weight_block_cart<LA, LB, LC, LD, T>(A, pb, pk, sc, W, lane);
+  __syncwarp(tmask);
+  const double ab[3] = {pb.abx, pb.aby, pb.abz};
+  const double cd[3] = {pk.abx, pk.aby, pk.abz};
+  constexpr int NE = LA + LB, NF = LC + LD;
+  constexpr int EA0 = LA > 0 ? LA - 1 : 0, FA0 = LC > 0 ? LC - 1 : 0;
+  constexpr int COLSP = nrange(FA0, NF), COLS1 = nrange(LC, NF), COLS2 = nrange(LC + 1, NF + 1);
+#pragma unroll 1
+  for (int q = 0; q < 9; ++q) g[q] = 0.0;
+  grad_shifted_ct<LA + 1, LB, LC, LD, 0, true, T>(slot + L.off_a, COLS1, 0, nrange(LA + 1, NE + 1), 0, W, buf, blk,
+                                                  ab, cd, g, lane, tmask);
+  if constexpr (LA > 0)
+    grad_shifted_ct<LA - 1, LB, LC, LD, 0, false, T>(slot + L.off_p, COLSP, 0, nrange(LA - 1, NE - 1),
+                                                     tri_below(LC) - tri_below(FA0), W, buf, blk, ab, cd, g, lane,
+                                                     tmask);
+  grad_shifted_ct<LA, LB + 1, LC, LD, 1, true, T>(slot + L.off_b, COLS1, 0, nrange(LA, NE + 1), 0, W, buf, blk, ab,
+                                                  cd, g + 3, lane, tmask);
+  if constexpr (LB > 0)
+    grad_shifted_ct<LA, LB - 1, LC, LD, 1, false, T>(slot + L.off_p, COLSP, tri_below(LA) - tri_below(EA0),
+                                                     nrange(LA, NE - 1), tri_below(LC) - tri_below(FA0), W, buf, blk,
+                                                     ab, cd, g + 3, lane, tmask);
+  grad_shifted_ct<LA, LB, LC + 1, LD, 2, true, T>(slot + L.off_c, COLS2, 0, nrange(LA, NE), 0, W, buf, blk, ab, cd,
+                                                  g + 6, lane, tmask);
+  if constexpr (LC > 0)
+    grad_shifted_ct<LA, LB, LC - 1, LD, 2, false, T>(slot + L.off_p, COLSP, tri_below(LA) - tri_below(EA0),
+                                                     nrange(LA, NE), 0, W, buf, blk, ab, cd, g + 6, lane, tmask);
+}
+
 // --------------------------------------------------------------- kernel
 
 template <int LA, int LB, int LC, int LD, typename R>
@@ -681,7 +816,10 @@ __global__ void __launch_bounds__(128) grad_kernel(KernelArgs A) {
         grad_team_passes<LA, LB, LC, LD, R, 0>(A, s_tab, pb, pk, sm, lane, tmask, slot);
       __syncwarp(tmask);
       double g[9];
-      grad_post(A, LA, LB, LC, LD, pb, pk, sc, slot, g, lane, T, tmask);
+      if (A.kinds == 0)
+        grad_post_cart<LA, LB, LC, LD, T>(A, pb, pk, sc, slot, g, lane, tmask);
+      else
+        grad_post(A, LA, LB, LC, LD, pb, pk, sc, slot, g, lane, T, tmask);
       if constexpr (T > 1) {
 #pragma unroll
         for (int q = 0; q < 9; ++q)
