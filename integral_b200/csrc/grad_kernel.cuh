@@ -91,15 +91,17 @@ __host__ __device__ inline GradSlot grad_slot_layout(int la, int lb, int lc, int
 }
 
 // Lanes per quartet: one thread while all accumulators fit in registers,
-// else the smallest team of 8, 16 or 32 lanes giving each lane at most two
-// rows of every segment.
+// else the smallest team of 8, 16 or 32 lanes giving each lane at most one
+// row of every segment (32 beyond that).  Measured against at most two rows
+// per lane: fewer columns per lane means fewer passes, each of which
+// recomputes the 2D tables of every primitive quartet.
 __host__ __device__ constexpr int grad_team_for(int la, int lb, int lc, int ld) {
   if (g_acc_total(la, lb, lc, ld) <= 40) return 1;
   int mr = 0;
   for (int s = 0; s < 3; ++s)
     if (g_nacc(la, lb, lc, ld, s) > 0 && g_rows(la, lb, lc, ld, s) > mr) mr = g_rows(la, lb, lc, ld, s);
   for (int t = 8; t < 32; t *= 2)
-    if ((mr + t - 1) / t <= 2) return t;
+    if ((mr + t - 1) / t <= 1) return t;
   return 32;
 }
 
@@ -167,7 +169,8 @@ struct GradShape {
   static constexpr int NR = (NE + NF + 1) / 2 + 1;
   static constexpr bool LOW = g_low(LA, LC);
   static constexpr int T = grad_team_for(LA, LB, LC, LD);
-  static constexpr int BUD = sizeof(R) == 8 ? 48 : 72;
+  // accumulators per lane per pass (measured: 80/112 beat 48/72 and 64/96)
+  static constexpr int BUD = sizeof(R) == 8 ? 80 : 112;
   static constexpr GradPassPlan PL = make_grad_plan(LA, LB, LC, LD, T, BUD);
   static constexpr int GT = (NEV + 1) * (NFV + 1);
   // per primitive quartet in shared memory: roots, weights*prefactor, the
