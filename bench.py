@@ -129,16 +129,30 @@ def grad_bench(args):
     print(json.dumps(line))
 
 
-def profile_case():
+def profile_case(workload="jk"):
     """One mixed J/K build of a 24-atom cut of the bench recipe (12-bohr
     cube): every class of the bench, inputs larger than L2 are not needed
-    because the kernels are compute bound; prints the launch records."""
+    because the kernels are compute bound; prints the launch records.  With
+    workload "grad": one FP64 gradient of a 16-atom cut of the gradient
+    recipe (12-bohr cube)."""
     import torch
 
     torch.cuda.set_device(0)
     import integral_b200 as ib
     from integral_b200 import systems as S
 
+    if workload == "grad":
+        s = S.grad_system(natom=16, side=12.0)
+        gc = ib.Basis(s["shells"]).direct_grad_contractor()
+        dens = gc.density([ib.GradDensityTerm(f, l, r) for f, l, r in s["coulomb"]],
+                          [ib.GradDensityTerm(f, l, r) for f, l, r in s["exchange"]])
+        gc.contract(dens, threshold=s["threshold"], precision=0)
+        st = gc.last_stats()
+        print(json.dumps({"case": "ERI gradient, 16 atoms, nao %d, FP64" % S.nao_of(s["shells"]),
+                          "quartets": st["quartets"], "kernel_ms": st["kernel_ms"]}))
+        for r in gc._plan.profile():
+            print(json.dumps(r))
+        return
     s = S.jk_system(natom=24, side=12.0)
     dc = ib.Basis(s["shells"]).direct_contractor()
     dc.jk(s["dens"], s["threshold"], precision=1)
@@ -295,7 +309,7 @@ def reference_arm(args):
 def main():
     args = parse()
     if args.profile_case:
-        return profile_case()
+        return profile_case(args.workload)
     if args.workload == "grad":
         return grad_bench(args)
     if args.impl == "reference":
