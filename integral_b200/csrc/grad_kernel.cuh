@@ -805,9 +805,11 @@ __global__ void __launch_bounds__(128) grad_kernel(KernelArgs A) {
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= A.task.total) break;
     const unsigned long long end = base + A.chunk < A.task.total ? base + A.chunk : A.task.total;
+    TaskCursor cur;
+    if (base + tw < end) cursor_seek(A.task, base + tw, cur);
     for (unsigned long long t = base + tw; t < end; t += TPW) {
       int pbi, pki;
-      decode_task(A.task, t, pbi, pki);
+      cursor_decode(A.task, t, cur, pbi, pki);
       const PairD pb = A.pairs[pbi];
       const PairD pk = A.pairs[pki];
       const Screen sc = screen_quartet(A, pb, pk);

@@ -53,6 +53,38 @@ __device__ __forceinline__ void decode_task(const TaskList& t, unsigned long lon
   pki = t.ket_pairs[kpos];
 }
 
+// Position in a task list: segment `seg` covers tasks [lo, hi).  A team
+// seeks once per claimed chunk (binary search) and then walks forward, its
+// tasks being increasing; the decode of every task equals decode_task's.
+struct TaskCursor {
+  int seg;
+  unsigned long long lo, hi;
+};
+__device__ __forceinline__ void cursor_seek(const TaskList& t, unsigned long long g, TaskCursor& c) {
+  int lo = 0, hi = t.nbra;  // prefix[lo] <= g < prefix[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (t.prefix[mid] <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  c.seg = lo;
+  c.lo = t.prefix[lo];
+  c.hi = t.prefix[lo + 1];
+}
+__device__ __forceinline__ void cursor_decode(const TaskList& t, unsigned long long g, TaskCursor& c, int& pbi,
+                                              int& pki) {
+  while (g >= c.hi) {  // g < prefix[nbra] = total, so seg stays below nbra
+    ++c.seg;
+    c.lo = c.hi;
+    c.hi = t.prefix[c.seg + 1];
+  }
+  const int kpos = (int)(g - c.lo) + (t.ket_start ? t.ket_start[c.seg] : 0);
+  pbi = t.bra_pair[c.seg];
+  pki = t.ket_pairs[kpos];
+}
+
 struct Screen {
   bool keep;
   bool swapped;       // reference bra is the evaluation ket pair

@@ -334,9 +334,11 @@ __global__ void __launch_bounds__(128, quartet_min_blocks<LA, LB, LC, LD>()) qua
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= A.task.total) break;
     const unsigned long long end = base + A.chunk < A.task.total ? base + A.chunk : A.task.total;
+    TaskCursor cur;
+    if (base + tw < end) cursor_seek(A.task, base + tw, cur);
     for (unsigned long long g = base + tw; g < end; g += TPW) {
       int pbi, pki;
-      decode_task(A.task, g, pbi, pki);
+      cursor_decode(A.task, g, cur, pbi, pki);
       const PairD pb = A.pairs[pbi];
       const PairD pk = A.pairs[pki];
       Screen sc = screen_quartet(A, pb, pk);
