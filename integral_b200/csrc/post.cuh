@@ -39,23 +39,10 @@ __host__ __device__ inline SlotLayout slot_layout(int la, int lb, int lc, int ld
   return L;
 }
 
-__device__ __forceinline__ void decode_task(const TaskList& t, unsigned long long g, int& pbi, int& pki) {
-  int lo = 0, hi = t.nbra;  // prefix[lo] <= g < prefix[hi]
-  while (hi - lo > 1) {
-    int mid = (lo + hi) >> 1;
-    if (t.prefix[mid] <= g)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  int kpos = (int)(g - t.prefix[lo]) + (t.ket_start ? t.ket_start[lo] : 0);
-  pbi = t.bra_pair[lo];
-  pki = t.ket_pairs[kpos];
-}
-
-// Position in a task list: segment `seg` covers tasks [lo, hi).  A team
-// seeks once per claimed chunk (binary search) and then walks forward, its
-// tasks being increasing; the decode of every task equals decode_task's.
+// Position in a task list: segment `seg` (one bra pair and a run of its
+// kets) covers tasks [lo, hi) with lo = prefix[seg].  A team seeks once per
+// claimed chunk (binary search) and then walks forward, its tasks being
+// increasing.  Task g is ket ket_start[seg] + (g - lo) of bra bra_pair[seg].
 struct TaskCursor {
   int seg;
   unsigned long long lo, hi;
@@ -394,24 +381,6 @@ __device__ __forceinline__ void jk_term(const double* B, const int dims[4], cons
     }
     if (w1 != 0.0) atomicAdd(T1 + (size_t)(offs[u] + iu) * nao + offs[v] + iv, w1 * acc);
     if (w2 != 0.0) atomicAdd(T2 + (size_t)(offs[v] + iv) * nao + offs[u] + iu, w2 * acc);
-  }
-}
-
-// Bra-block J term accumulated across consecutive quartets of one bra pair
-// (the J' entries of the evaluation bra block change only when the bra does):
-// acc[q] += w * sum_{cd} B[ab cd] D[C c][D d], flushed by flush_bra_acc.
-__device__ __forceinline__ void jk_term_acc(const double* B, const int dims[4], const int offs[4], int nao,
-                                            const double* Dm, double w, double* acc, int lane, int T) {
-  const int st1 = dims[2] * dims[3];
-  const int nu = dims[0], nv = dims[1], ns = dims[2], nt = dims[3];
-  for (int q = lane; q < nu * nv; q += T) {
-    const double* row = B + (size_t)q * st1;
-    double s = 0.0;
-    for (int is = 0; is < ns; ++is) {
-      const double* drow = Dm + (size_t)(offs[2] + is) * nao + offs[3];
-      for (int it = 0; it < nt; ++it) s += row[is * nt + it] * __ldg(drow + it);
-    }
-    acc[q] += w * s;
   }
 }
 
