@@ -139,3 +139,23 @@ def test_two_rank_sharded_jk_equals_single_rank(tmp_path):
     assert int(r["count"][0]) == cnt
     assert float(np.max(np.abs(r["J"] - J))) < 1e-12 * float(np.max(np.abs(J)))
     assert float(np.max(np.abs(r["K"] - K))) < 1e-12 * float(np.max(np.abs(K)))
+
+
+def test_bench_reference_arm_prints_the_contract_line():
+    """bench.py --impl reference (the reference algorithm on the host cores,
+    via the C++ restatement) prints one JSON line with the contract's keys."""
+    import json
+    import subprocess
+    import sys
+
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0", "--cpu-sample-bras", "12"], capture_output=True, text=True, timeout=600,
+                         cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    for k in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in line, k
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0
