@@ -139,6 +139,15 @@ int igpu_eri_dense(igpu_plan* plan, double* out);
  * ket pairs scattered into the 4 bra/ket-internal slots of the host nao^4
  * buffer (assigned; other elements untouched). */
 int igpu_eri_builder_fill(igpu_plan* plan, const uint32_t* bra_subset, size_t nsub, double* out);
+/* PackedEriBuilder::build / fill (src/packed_eri.rs:156-237): the
+ * symmetry-unique tensor, AO pairs numbered shell-pair blocked (canonical
+ * shell pair, then (a, b) row-major with b <= a on diagonal pairs, see
+ * packed_eri.rs:10-21), element (t|u), u <= t, at t(t+1)/2 + u; m(m+1)/2
+ * doubles for m = nao(nao+1)/2.  Writes every canonical quartet with a bra
+ * in bra_subset (all when NULL) into `out` (host, caller-initialised; other
+ * elements are left as they are).  threshold > 0 skips quartets with
+ * Q_ij*Q_kl < threshold; threshold <= 0 screens nothing. */
+int igpu_eri_packed(igpu_plan* plan, double threshold, const uint32_t* bra_subset, size_t nsub, double* out);
 
 /* DirectContractor::density_shell_bounds (direct.rs:103-125): per density the
  * max |D| of every ordered shell block, ndens x nsh x nsh. */

@@ -235,6 +235,9 @@ class Basis:
     def direct_grad_contractor(self) -> "DirectGradContractor":
         return DirectGradContractor(self)
 
+    def packed_eri_builder(self) -> "PackedEriBuilder":
+        return PackedEriBuilder(self)
+
 
 # ------------------------------------------------------------ EriBuilder
 
@@ -287,6 +290,91 @@ class EriBuilder:
     def build(self) -> np.ndarray:
         out = np.zeros(self.output_len())
         _lib.check(_lib.lib().igpu_eri_builder_fill(self._plan.h, None, 0, out.ctypes.data_as(c_double_p)))
+        return out
+
+
+class PackedEriWorkspace:
+    """Worker-local scratch of the reference (src/packed_eri.rs:36-50); the
+    device plan keeps its own, kept for API parity."""
+
+
+@dataclass
+class PackedBraFill:
+    """One task of PackedEriBuilder.partition: the canonical bra pair and its
+    contiguous row range of the packed tensor (`rows`, a view of `out`)."""
+    bra: int
+    rows: np.ndarray
+    out: np.ndarray
+
+
+class PackedEriBuilder:
+    """The symmetry-unique ERI tensor (src/packed_eri.rs): each canonical
+    shell quartet evaluated once, stored as the lower triangle over AO-pair
+    indices numbered shell-pair blocked (canonical shell pair (i >= j), then
+    (a, b) row-major with b <= a when i == j); (t|u), u <= t, at
+    t(t+1)/2 + u."""
+
+    def __init__(self, basis: Basis, engine: Engine = Engine.Auto):
+        self._plan = basis.plan(engine)
+        sh = basis.shells()
+        offs = basis.offsets()
+        nsh = len(sh)
+        self._pairs = [(i, j) for i in range(nsh) for j in range(i + 1)]
+        self._ao_pairs = []
+        self._start = []
+        for i, j in self._pairs:
+            self._start.append(len(self._ao_pairs))
+            for a in range(sh[i].n_func()):
+                for b in range(a + 1 if i == j else sh[j].n_func()):
+                    self._ao_pairs.append((offs[i] + a, offs[j] + b))
+        self._start.append(len(self._ao_pairs))
+
+    @classmethod
+    def new(cls, basis):
+        return cls(basis)
+
+    @classmethod
+    def with_engine(cls, basis, engine):
+        return cls(basis, engine)
+
+    def bra_pairs(self):
+        return list(self._pairs)
+
+    def ao_pairs(self):
+        return list(self._ao_pairs)
+
+    def output_len(self) -> int:
+        m = len(self._ao_pairs)
+        return m * (m + 1) // 2
+
+    def partition(self, out: np.ndarray):
+        if out.size != self.output_len():
+            raise IntegralError(-7, "length mismatch",
+                                "packed ERI output buffer must hold %d elements" % self.output_len())
+        tasks = []
+        for bra in range(len(self._pairs)):
+            lo, hi = self._start[bra], self._start[bra + 1]
+            tasks.append(PackedBraFill(bra, out[lo * (lo + 1) // 2: hi * (hi + 1) // 2], out))
+        return tasks
+
+    def fill(self, workspace, task: PackedBraFill, threshold: float):
+        self.fill_many([task], threshold)
+
+    def fill_many(self, tasks: Sequence[PackedBraFill], threshold: float):
+        """Fill several tasks of one output buffer in one launch sequence."""
+        if not tasks:
+            return
+        out = tasks[0].out
+        if not out.flags["C_CONTIGUOUS"] or out.dtype != np.float64:
+            raise IntegralError(-1, "invalid argument", "output must be contiguous float64")
+        idx = np.ascontiguousarray([t.bra for t in tasks], dtype=np.uint32)
+        _lib.check(_lib.lib().igpu_eri_packed(self._plan.h, float(threshold), idx.ctypes.data_as(c_u32_p),
+                                              len(idx), out.ctypes.data_as(c_double_p)))
+
+    def build(self, threshold: float) -> np.ndarray:
+        out = np.zeros(self.output_len())
+        _lib.check(_lib.lib().igpu_eri_packed(self._plan.h, float(threshold), None, 0,
+                                              out.ctypes.data_as(c_double_p)))
         return out
 
 

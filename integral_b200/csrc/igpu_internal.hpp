@@ -94,6 +94,7 @@ enum Mode : int {
   MODE_SCHWARZ = 2,
   MODE_BUILDER = 3,
   MODE_GRAD = 4,
+  MODE_PACKED = 5,
 };
 
 struct JKDev {
@@ -153,7 +154,8 @@ struct KernelArgs {
   size_t slot_doubles;
   JKDev jk;
   GradDev grad;
-  double* dense;         // nao^4 (MODE_DENSE / MODE_BUILDER)
+  double* dense;         // nao^4 (MODE_DENSE / MODE_BUILDER); packed triangle (MODE_PACKED)
+  const long long* packed_start;  // MODE_PACKED: first AO-pair index of every canonical shell pair
   double* schwarz_out;   // per pair Q (MODE_SCHWARZ)
   Counters* counters;
   int builder_swap;      // builder mode: requested bra is the evaluation ket

@@ -140,6 +140,8 @@ struct igpu_plan {
   // gradient: term matrices, their block maxima and the device term tables
   DevBuf<double> d_gmat, d_gmax, d_gfac, d_gout;
   DevBuf<const double*> d_gptr;
+  // packed tensor: first AO-pair index of every canonical shell pair
+  DevBuf<long long> d_packed_start;
 };
 
 namespace {
@@ -1017,6 +1019,73 @@ int igpu_eri_dense(igpu_plan* P, double* out) { return dense_like(P, false, null
 
 int igpu_eri_builder_fill(igpu_plan* P, const uint32_t* sub, size_t nsub, double* out) {
   return dense_like(P, true, sub, nsub, out);
+}
+
+int igpu_eri_packed(igpu_plan* P, double threshold, const uint32_t* sub, size_t nsub, double* out) {
+  if (!P || !out) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (std::isnan(threshold)) return fail(IGPU_ERR_INVALID_ARGUMENT, "threshold is NaN");
+  // shell-pair blocked AO-pair numbering (packed_eri.rs:103-114)
+  std::vector<long long> start(P->npairs + 1, 0);
+  for (int p = 0; p < P->npairs; ++p) {
+    const int ni = P->shells[P->pairs[p].i].nfunc, nj = P->shells[P->pairs[p].j].nfunc;
+    start[p + 1] = start[p] + (P->pairs[p].i == P->pairs[p].j ? (long long)ni * (ni + 1) / 2 : (long long)ni * nj);
+  }
+  const size_t m = (size_t)start[P->npairs];
+  const size_t len = m * (m + 1) / 2;
+  std::vector<unsigned> bitmap;
+  if (sub) {
+    int rc = check_bra_subset(P, sub, nsub, bitmap);
+    if (rc) return rc;
+  }
+  cudaStream_t s = P->stream;
+  CK(P->d_packed_start.upload(start, s));
+  if (P->d_dense.ensure(len) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(IGPU_ERR_OUT_OF_MEMORY, "packed tensor of " + std::to_string(len) + " doubles does not fit");
+  }
+  // the caller's buffer is the initial content: rows of other bras stay
+  CK(cudaMemcpyAsync(P->d_dense.p, out, len * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (sub) {
+    CK(P->d_bitmap.ensure(bitmap.size()));
+    CK(cudaMemcpyAsync(P->d_bitmap.p, bitmap.data(), bitmap.size() * sizeof(unsigned), cudaMemcpyHostToDevice, s));
+  }
+  // threshold > 0: skip Q_ij*Q_kl < threshold (packed_eri.rs:184-187);
+  // otherwise every canonical quartet
+  TaskSet* ts = nullptr;
+  int rc = IGPU_OK;
+  if (threshold > 0.0) {
+    auto key = std::make_pair(threshold, 0.0);
+    auto it = P->jk_tasks.find(key);
+    if (it == P->jk_tasks.end()) {
+      auto t = std::make_unique<TaskSet>();
+      rc = build_jk_tasks(P, threshold, 0.0, *t);
+      if (rc) return rc;
+      CK(cudaStreamSynchronize(P->stream));
+      it = P->jk_tasks.emplace(key, std::move(t)).first;
+    }
+    ts = it->second.get();
+  } else {
+    if (!P->dense_tasks) {
+      P->dense_tasks = std::make_unique<TaskSet>();
+      rc = build_jk_tasks(P, -std::numeric_limits<double>::infinity(), 0.0, *P->dense_tasks);
+      if (rc) return rc;
+    }
+    ts = P->dense_tasks.get();
+  }
+  KernelArgs A = base_args(P);
+  A.mode = MODE_PACKED;
+  A.dense = P->d_dense.p;
+  A.packed_start = P->d_packed_start.p;
+  A.bra_bitmap = sub ? P->d_bitmap.p : nullptr;
+  A.counters = nullptr;
+  uint32_t launches = 0;
+  rc = run_tasks(P, *ts, A, s, launches);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(out, P->d_dense.p, len * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  P->last = igpu_stats{};
+  P->last.launches = launches;
+  return IGPU_OK;
 }
 
 int igpu_last_stats(const igpu_plan* P, igpu_stats* st) {

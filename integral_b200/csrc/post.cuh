@@ -601,6 +601,42 @@ __device__ __forceinline__ void consume_builder(const KernelArgs& A, const doubl
   }
 }
 
+// Packed symmetry-unique tensor (src/packed_eri.rs:10-21, 297-327): AO pairs
+// numbered shell-pair blocked (canonical shell pair, then (a, b) row-major
+// with b <= a when i == j), element (t|u), u <= t, at t(t+1)/2 + u.  The block
+// is taken in the reference orientation (i,j|k,l) of the canonical quartet,
+// bra = the pair with the larger canonical index; every unique element is
+// written once.
+__device__ __forceinline__ void consume_packed(const KernelArgs& A, const double* B, const int dims[4],
+                                               const PairD& pb, const PairD& pk, const Screen& sc, int lane, int T) {
+  const PairD& rb = sc.swapped ? pk : pb;
+  const PairD& rk = sc.swapped ? pb : pk;
+  // evaluation slot of reference positions i, j, k, l
+  const bool bflip = pb.a != pb.i, kflip = pk.a != pk.i;
+  const int e0 = !sc.swapped ? (bflip ? 1 : 0) : (kflip ? 3 : 2);
+  const int e1 = !sc.swapped ? (bflip ? 0 : 1) : (kflip ? 2 : 3);
+  const int e2 = !sc.swapped ? (kflip ? 3 : 2) : (bflip ? 1 : 0);
+  const int e3 = !sc.swapped ? (kflip ? 2 : 3) : (bflip ? 0 : 1);
+  auto pick = [](int e, int x0, int x1, int x2, int x3) { return e == 0 ? x0 : (e == 1 ? x1 : (e == 2 ? x2 : x3)); };
+  const int nj = pick(e1, dims[0], dims[1], dims[2], dims[3]);
+  const int nl = pick(e3, dims[0], dims[1], dims[2], dims[3]);
+  const bool bra_diag = rb.i == rb.j, ket_diag = rk.i == rk.j, same = rb.tri == rk.tri;
+  const long long t0 = A.packed_start[rb.tri], u0 = A.packed_start[rk.tri];
+  const int total = dims[0] * dims[1] * dims[2] * dims[3];
+  for (int q = lane; q < total; q += T) {
+    const int f3 = q % dims[3], f2 = (q / dims[3]) % dims[2], f1 = (q / (dims[3] * dims[2])) % dims[1],
+              f0 = q / (dims[3] * dims[2] * dims[1]);
+    const int a = pick(e0, f0, f1, f2, f3), b = pick(e1, f0, f1, f2, f3);
+    const int c = pick(e2, f0, f1, f2, f3), d = pick(e3, f0, f1, f2, f3);
+    if (bra_diag && b > a) continue;
+    if (ket_diag && d > c) continue;
+    const long long t = t0 + (bra_diag ? (long long)a * (a + 1) / 2 + b : (long long)a * nj + b);
+    const long long u = u0 + (ket_diag ? (long long)c * (c + 1) / 2 + d : (long long)c * nl + d);
+    if (same && u > t) continue;
+    A.dense[(size_t)t * (size_t)(t + 1) / 2 + (size_t)u] = B[q];
+  }
+}
+
 // Schwarz: sqrt(max |(mu nu|mu nu)|) over the function-space diagonal of the
 // (ij|ij) block (src/integrals.rs:850-860).
 __device__ __forceinline__ void consume_schwarz(const KernelArgs& A, const double* B, const int dims[4],
@@ -647,6 +683,9 @@ __device__ __forceinline__ void post_quartet(const KernelArgs& A, const ClassDim
       break;
     case MODE_BUILDER:
       consume_builder(A, B, dims, offs, shl, A.builder_swap != 0, lane, T);
+      break;
+    case MODE_PACKED:
+      consume_packed(A, B, dims, pb, pk, sc, lane, T);
       break;
     case MODE_SCHWARZ:
       consume_schwarz(A, B, dims, pb_index, lane, T, tmask);
