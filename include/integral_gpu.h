@@ -130,6 +130,14 @@ int igpu_atoms(const igpu_plan* plan, double* xyz);
 int igpu_schwarz(const igpu_plan* plan, double* q);
 /* Plan cutoff for IGPU_PRECISION_MIXED (default 1e-4). */
 int igpu_set_mixed_cutoff(igpu_plan* plan, double cutoff);
+/* EriKernel (src/integrals.rs:304-321) of every later call on the plan:
+ * omega = 0 is Coulomb 1/r (the default); omega > 0 finite is the long-range
+ * erf(omega r)/r (Basis::eri_kernel, EriBuilder::kernel, the gradient's
+ * kernel argument).  The J/K entries apply it too, with no counterpart in
+ * the reference (its DirectContractor is Coulomb only).  Screening keeps the
+ * Coulomb Schwarz bounds, which bound the attenuated integrals.  Any other
+ * omega is IGPU_ERR_INVALID_ARGUMENT (the reference's check_erf_omega). */
+int igpu_set_erf_omega(igpu_plan* plan, double omega);
 
 /* Basis::eri / eri_with (integrals.rs:664-754): dense nao^4 tensor into a
  * host buffer of nao^4 doubles (assigned). */

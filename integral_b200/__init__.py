@@ -62,6 +62,33 @@ class Engine(enum.IntEnum):
     Rys = 2
 
 
+class EriKernel:
+    """Two-electron operator (src/integrals.rs:304-312): EriKernel.Coulomb
+    (1/r12) or EriKernel.Erf(omega) (the long-range erf(omega r12)/r12,
+    omega finite and > 0)."""
+
+    Coulomb = None  # set below
+
+    def __init__(self, omega: float = 0.0):
+        self.omega = float(omega)
+
+    @classmethod
+    def Erf(cls, omega: float) -> "EriKernel":
+        if not (omega > 0.0 and np.isfinite(omega)):
+            raise IntegralError(-1, "invalid argument", "EriKernel::Erf requires a finite omega > 0")
+        return cls(omega)
+
+    def __repr__(self):
+        return "EriKernel.Coulomb" if self.omega == 0.0 else "EriKernel.Erf(omega=%r)" % self.omega
+
+
+EriKernel.Coulomb = EriKernel(0.0)
+
+
+def _omega_of(kernel) -> float:
+    return 0.0 if kernel is None else float(kernel.omega)
+
+
 def n_cart(l: int) -> int:
     return (l + 1) * (l + 2) // 2
 
@@ -126,6 +153,10 @@ class Shell:
 
 class _Plan:
     """Owner of one igpu_plan (device-resident precompute)."""
+
+    def set_erf_omega(self, omega: float):
+        """Operator of later calls: 0 Coulomb, > 0 erf(omega r)/r."""
+        _lib.check(_lib.lib().igpu_set_erf_omega(self.h, float(omega)))
 
     def __init__(self, shells: Sequence[Shell], engine: Engine):
         L = _lib.lib()
@@ -216,6 +247,19 @@ class Basis:
     def eri(self) -> np.ndarray:
         return self.eri_with(Engine.Auto)
 
+    def eri_kernel(self, kernel: "EriKernel") -> np.ndarray:
+        """Basis::eri_kernel (src/integrals.rs:773-820): the dense tensor of
+        the given operator (Coulomb or long-range erf)."""
+        p = self.plan(Engine.Auto)
+        p.set_erf_omega(_omega_of(kernel))
+        try:
+            n = p.nao
+            out = np.empty(n ** 4)
+            _lib.check(_lib.lib().igpu_eri_dense(p.h, out.ctypes.data_as(c_double_p)))
+        finally:
+            p.set_erf_omega(0.0)
+        return out
+
     def eri_with(self, engine: Engine) -> np.ndarray:
         p = self.plan(engine)
         n = p.nao
@@ -257,16 +301,30 @@ class EriBuilder:
         self._basis = basis
         self._plan = basis.plan(engine)
         self._pairs = self._plan.bra_pairs()
+        self._omega = 0.0
 
     @classmethod
     def with_engine(cls, basis, engine):
         return cls(basis, engine)
+
+    def kernel(self, k: "EriKernel") -> "EriBuilder":
+        """EriBuilder::kernel (src/eri_builder.rs:280-304): the operator the
+        later fills evaluate; builder-style, returns self."""
+        self._omega = _omega_of(k)
+        return self
 
     def bra_pairs(self):
         return list(self._pairs)
 
     def output_len(self) -> int:
         return self._plan.nao ** 4
+
+    def _run(self, idx, n, out):
+        self._plan.set_erf_omega(self._omega)
+        try:
+            _lib.check(_lib.lib().igpu_eri_builder_fill(self._plan.h, idx, n, out.ctypes.data_as(c_double_p)))
+        finally:
+            self._plan.set_erf_omega(0.0)
 
     def partition(self, out: np.ndarray):
         if out.size != self.output_len():
@@ -284,12 +342,11 @@ class EriBuilder:
         if not out.flags["C_CONTIGUOUS"] or out.dtype != np.float64:
             raise IntegralError(-1, "invalid argument", "output must be contiguous float64")
         idx = np.ascontiguousarray([t.index for t in tasks], dtype=np.uint32)
-        _lib.check(_lib.lib().igpu_eri_builder_fill(self._plan.h, idx.ctypes.data_as(c_u32_p), len(idx),
-                                                     out.ctypes.data_as(c_double_p)))
+        self._run(idx.ctypes.data_as(c_u32_p), len(idx), out)
 
     def build(self) -> np.ndarray:
         out = np.zeros(self.output_len())
-        _lib.check(_lib.lib().igpu_eri_builder_fill(self._plan.h, None, 0, out.ctypes.data_as(c_double_p)))
+        self._run(None, 0, out)
         return out
 
 
@@ -577,7 +634,7 @@ class DirectGradContractor:
         return arr, keep
 
     def accumulate_bra_pairs(self, workspace, bra_indices, density: GradDensity, threshold: float, out: np.ndarray,
-                             precision: int = 0):
+                             precision: int = 0, kernel: "EriKernel" = None):
         if density.nao != self._plan.nao:
             raise IntegralError(-1, "invalid argument", "density prepared for a different plan")
         if out.shape != (self._plan.natom, 3):
@@ -586,21 +643,25 @@ class DirectGradContractor:
         xa, k2 = self._terms(density.exchange)
         res = np.zeros(self._plan.natom * 3)
         sub = None if bra_indices is None else np.ascontiguousarray(bra_indices, dtype=np.uint32)
-        _lib.check(_lib.lib().igpu_grad(
-            self._plan.h, ca, len(density.coulomb), xa, len(density.exchange),
-            sub.ctypes.data_as(c_u32_p) if sub is not None else None, 0 if sub is None else len(sub),
-            float(threshold), int(precision), res.ctypes.data_as(c_double_p)))
+        self._plan.set_erf_omega(_omega_of(kernel))
+        try:
+            _lib.check(_lib.lib().igpu_grad(
+                self._plan.h, ca, len(density.coulomb), xa, len(density.exchange),
+                sub.ctypes.data_as(c_u32_p) if sub is not None else None, 0 if sub is None else len(sub),
+                float(threshold), int(precision), res.ctypes.data_as(c_double_p)))
+        finally:
+            self._plan.set_erf_omega(0.0)
         out += res.reshape(-1, 3)
 
     def accumulate_bra_pair(self, workspace, bra, density, kernel, threshold, out):
         i, j = bra
         if j > i:
             raise IntegralError(-8, "non-canonical bra pair", "bra must satisfy i >= j")
-        self.accumulate_bra_pairs(workspace, [i * (i + 1) // 2 + j], density, threshold, out)
+        self.accumulate_bra_pairs(workspace, [i * (i + 1) // 2 + j], density, threshold, out, kernel=kernel)
 
     def contract(self, density: GradDensity, kernel=None, threshold: float = 0.0, precision: int = 0) -> np.ndarray:
         out = np.zeros((self._plan.natom, 3))
-        self.accumulate_bra_pairs(DirectGradWorkspace(), None, density, threshold, out, precision)
+        self.accumulate_bra_pairs(DirectGradWorkspace(), None, density, threshold, out, precision, kernel=kernel)
         return out
 
     def last_stats(self) -> dict:

@@ -262,17 +262,23 @@ __device__ __forceinline__ void vrr_axis(R g00, R c00, R cp0, R b10, R b01, R b0
 }
 
 // Per-primitive-quartet scalars of the Rys quadrature (src/engine/rys.rs:
-// 140-166) in evaluation orientation.
+// 140-166) in evaluation orientation.  For the long-range operator
+// erf(omega r)/r (omega > 0, src/engine/rys.rs:163-175) the quadrature is
+// taken at s*T with s = omega^2 / (rho + omega^2), every root scaled by s
+// (xs) and every weight by sqrt(s) (folded into pref); omega = 0 is the
+// Coulomb operator, with T and pref untouched and xs = 1.
 template <typename R>
 struct QuartetHdr {
   R T, pref, pq, p, q;
   R pqx, pqy, pqz;  // P - Q
   R pax, pay, paz;  // P - A
   R qcx, qcy, qcz;  // Q - C
+  R xs;             // root scale (1 for Coulomb)
 };
 
 template <typename R>
-__device__ __forceinline__ QuartetHdr<R> quartet_header(const PrimPairD& bp, const PrimPairD& kp) {
+__device__ __forceinline__ QuartetHdr<R> quartet_header(const PrimPairD& bp, const PrimPairD& kp,
+                                                        double omega) {
   QuartetHdr<R> h;
   // 2 pi^{5/2}
   const double TWO_PI_2_5 = 34.98683665524972;
@@ -294,6 +300,14 @@ __device__ __forceinline__ QuartetHdr<R> quartet_header(const PrimPairD& bp, con
   h.qcx = R(kp.pax);
   h.qcy = R(kp.pay);
   h.qcz = R(kp.paz);
+  h.xs = R(1);
+  if (omega > 0.0) {
+    const R w2 = R(omega) * R(omega);
+    const R sc = w2 / (rho + w2);
+    h.T *= sc;
+    h.pref *= sqrt(sc);
+    h.xs = sc;
+  }
   return h;
 }
 

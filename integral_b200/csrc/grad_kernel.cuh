@@ -210,7 +210,7 @@ __device__ __forceinline__ void grad_tables_thread(const KernelArgs& A, const R*
     for (int kq = 0; kq < pk.nprim; ++kq) {
       const PrimPairD kp = A.prims[pk.prim_off + kq];
       const R wC = R(2) * R(kp.alpha);
-      const QuartetHdr<R> h = quartet_header<R>(bp, kp);
+      const QuartetHdr<R> h = quartet_header<R>(bp, kp, A.omega);
       R x[NR], w[NR];
       rys_roots_s<NR, R>(s_tab, h.T, x, w);
       const R inv_pq = R(1) / h.pq;
@@ -218,7 +218,7 @@ __device__ __forceinline__ void grad_tables_thread(const KernelArgs& A, const R*
       const R inv2pq = R(0.5) * inv_pq, inv2p = R(0.5) / h.p, inv2q = R(0.5) / h.q;
 #pragma unroll
       for (int r = 0; r < NR; ++r) {
-        const R xr = x[r];
+        const R xr = x[r] * h.xs;
         const R b00 = xr * inv2pq;
         const R b10 = (R(1) - xr * qpq) * inv2p;
         const R b01 = (R(1) - xr * ppq) * inv2q;
@@ -319,11 +319,11 @@ __device__ __forceinline__ void grad_team_pass(const KernelArgs& A, const R* s_t
       const int ip = pidx / npk, kq = pidx - ip * npk;
       const PrimPairD bp = A.prims[pb.prim_off + ip];
       const PrimPairD kp = A.prims[pk.prim_off + kq];
-      h = quartet_header<R>(bp, kp);
+      h = quartet_header<R>(bp, kp, A.omega);
       for (int r = sub; r < NR; r += SUB) {
         R xr, wr;
         rys_root_one<NR, R>(s_tab, h.T, r, xr, wr);
-        mys[r] = xr;
+        mys[r] = xr * h.xs;
         mys[NR + r] = wr * h.pref;
       }
       if (sub == 0) {

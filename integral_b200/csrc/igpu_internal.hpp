@@ -164,6 +164,7 @@ struct KernelArgs {
   unsigned long long chunk;          // tasks claimed per grab (per warp)
   size_t acc_offset;     // slot offset of the running bra-block J accumulators
   int kinds;             // 0 all shells Cartesian, 1 all spherical, 2 mixed
+  double omega;          // 0: Coulomb 1/r; > 0: long-range erf(omega r)/r
 };
 
 }  // namespace igpu

@@ -131,6 +131,7 @@ struct igpu_plan {
   std::map<std::pair<double, double>, std::unique_ptr<TaskSet>> jk_tasks;  // (threshold, fp64 cutoff)
   std::unique_ptr<TaskSet> dense_tasks;
   double mixed_cutoff = 1e-4;
+  double erf_omega = 0.0;  // 0: Coulomb; > 0: erf(omega r)/r for every later call
   bool all_spherical = false;
   igpu_stats last{};
   DevBuf<Counters> d_launch_counters;
@@ -208,6 +209,7 @@ KernelArgs base_args(igpu_plan* P) {
   A.nao = P->nao;
   A.counters = P->d_counters.p;
   A.kinds = P->all_spherical ? 1 : (P->spherical_any ? 2 : 0);
+  A.omega = P->erf_omega;
   return A;
 }
 
@@ -499,6 +501,7 @@ int run_schwarz(igpu_plan* P) {
   CK(P->d_schwarz_pair.ensure(P->npairs));
   KernelArgs A = base_args(P);
   A.mode = MODE_SCHWARZ;
+  A.omega = 0.0;  // Coulomb bounds (they bound the attenuated integrals too)
   A.schwarz_out = P->d_schwarz_pair.p;
   A.counters = nullptr;
   uint32_t launches = 0;
@@ -733,6 +736,15 @@ int igpu_atoms(const igpu_plan* P, double* xyz) {
 int igpu_schwarz(const igpu_plan* P, double* q) {
   if (!P || !q) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
   std::memcpy(q, P->schwarz.data(), P->schwarz.size() * sizeof(double));
+  return IGPU_OK;
+}
+
+int igpu_set_erf_omega(igpu_plan* P, double omega) {
+  // check_erf_omega (src/integrals.rs:316-321): finite and > 0; 0 = Coulomb
+  if (!P) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!(omega == 0.0 || (omega > 0.0 && std::isfinite(omega))))
+    return fail(IGPU_ERR_INVALID_ARGUMENT, "EriKernel::Erf requires a finite omega > 0");
+  P->erf_omega = omega;
   return IGPU_OK;
 }
 

@@ -97,7 +97,7 @@ __device__ __forceinline__ void accumulate_thread(const KernelArgs& A, const R* 
     const PrimPairD bp = A.prims[pb.prim_off + ip];
     for (int kq = 0; kq < pk.nprim; ++kq) {
       const PrimPairD kp = A.prims[pk.prim_off + kq];
-      const QuartetHdr<R> h = quartet_header<R>(bp, kp);
+      const QuartetHdr<R> h = quartet_header<R>(bp, kp, A.omega);
       R x[NR], w[NR];
       rys_roots_s<NR, R>(s_tab, h.T, x, w);
       const R inv_pq = R(1) / h.pq;
@@ -105,7 +105,7 @@ __device__ __forceinline__ void accumulate_thread(const KernelArgs& A, const R* 
       const R inv2pq = R(0.5) * inv_pq, inv2p = R(0.5) / h.p, inv2q = R(0.5) / h.q;
 #pragma unroll
       for (int r = 0; r < NR; ++r) {
-        const R xr = x[r];
+        const R xr = x[r] * h.xs;
         const R b00 = xr * inv2pq;
         const R b10 = (R(1) - xr * qpq) * inv2p;
         const R b01 = (R(1) - xr * ppq) * inv2q;
@@ -197,11 +197,11 @@ __device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, c
     if (active) {
       const int pidx = base + myp;
       const int ip = pidx / npk, kq = pidx - ip * npk;
-      h = quartet_header<R>(A.prims[pb.prim_off + ip], A.prims[pk.prim_off + kq]);
+      h = quartet_header<R>(A.prims[pb.prim_off + ip], A.prims[pk.prim_off + kq], A.omega);
       for (int r = sub; r < NR; r += SUB) {
         R xr, wr;
         rys_root_one<NR, R>(s_tab, h.T, r, xr, wr);
-        mys[r] = xr;
+        mys[r] = xr * h.xs;
         mys[NR + r] = wr * h.pref;
       }
     }

@@ -56,6 +56,8 @@ void orc_basis_free(void* b) { delete static_cast<Basis*>(b); }
 int orc_nao(void* b) { return static_cast<Basis*>(b)->nao(); }
 int orc_natom(void* b) { return (int)static_cast<Basis*>(b)->atoms().size(); }
 
+void orc_set_erf_omega(double omega) { set_rys_erf_omega(omega); }
+
 void orc_eri(void* b, int engine, double* out) {
   std::vector<double> e = static_cast<Basis*>(b)->eri((Engine)engine);
   std::memcpy(out, e.data(), e.size() * sizeof(double));

@@ -351,6 +351,12 @@ void build_axis(int la, int lb, int lc, int ld, double c00, double cp0, double b
 }
 }  // namespace
 
+namespace {
+double g_rys_erf_omega = 0.0;
+}
+void set_rys_erf_omega(double omega) { g_rys_erf_omega = omega; }
+double rys_erf_omega() { return g_rys_erf_omega; }
+
 void rys_prim_quartet(double ea, const Vec3& A, int la, double eb, const Vec3& B, int lb,
                       double ec, const Vec3& C, int lc, double ed, const Vec3& D, int ld,
                       double scale, double* out) {
@@ -369,7 +375,18 @@ void rys_prim_quartet(double ea, const Vec3& A, int la, double eb, const Vec3& B
   int l_total = la + lb + lc + ld;
   int nroots = l_total / 2 + 1;
   double roots[MAX_RYS_ROOTS], wts[MAX_RYS_ROOTS];
-  rys_roots_weights(nroots, t, roots, wts);
+  const double omega = rys_erf_omega();
+  if (omega > 0.0) {
+    // erf(omega r)/r (crates/integral/src/engine/rys.rs:163-175): quadrature at s*T, roots
+    // scaled by s, weights by sqrt(s)
+    double s = omega * omega / (rho + omega * omega);
+    rys_roots_weights(nroots, s * t, roots, wts);
+    double sqrt_s = std::sqrt(s);
+    for (int r = 0; r < nroots; ++r) roots[r] *= s;
+    for (int r = 0; r < nroots; ++r) wts[r] *= sqrt_s;
+  } else {
+    rys_roots_weights(nroots, t, roots, wts);
+  }
   Vec3 pa = sub(p_ctr, A), qc = sub(q_ctr, C), ab = sub(A, B), cd = sub(C, D);
   const auto& tri = tri_all();
   const std::vector<Tri>&ca = tri[la], &cb = tri[lb], &cc = tri[lc], &cdv = tri[ld];

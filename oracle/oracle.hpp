@@ -100,6 +100,11 @@ std::vector<PrimPair> build_pairs(const Shell& s1, const double* c1, const Shell
 void os_shell_quartet(const Shell& a, const Shell& b, const Shell& c, const Shell& d,
                       const std::vector<PrimPair>& bra, const std::vector<PrimPair>& ket,
                       int la, int lb, int lc, int ld, double* out);
+// Operator of the Rys primitive quartets below (process-wide, test use):
+// 0 = Coulomb, > 0 = erf(omega r)/r (src/engine/rys.rs:101-172).  The OS/HGP
+// engine has no attenuated path (as in the reference): erf callers use Rys.
+void set_rys_erf_omega(double omega);
+double rys_erf_omega();
 // Rys primitive quartet (src/engine/rys.rs:121-231).
 void rys_prim_quartet(double ea, const Vec3& A, int la, double eb, const Vec3& B, int lb,
                       double ec, const Vec3& C, int lc, double ed, const Vec3& D, int ld,

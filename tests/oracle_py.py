@@ -45,6 +45,7 @@ def lib():
         L.orc_nao.argtypes = [ctypes.c_void_p]
         L.orc_natom.argtypes = [ctypes.c_void_p]
         L.orc_eri.argtypes = [ctypes.c_void_p, ctypes.c_int, c_double_p]
+        L.orc_set_erf_omega.argtypes = [ctypes.c_double]
         L.orc_eri_block.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_int] * 4 + [c_double_p]
         L.orc_schwarz.argtypes = [ctypes.c_void_p, ctypes.c_int, c_double_p]
         L.orc_direct_new.restype = ctypes.c_void_p
@@ -117,6 +118,12 @@ class OracleBasis:
                 L.orc_basis_free(self.h)
         except Exception:
             pass
+
+    def eri_erf(self, omega):
+        """Dense tensor of erf(omega r)/r (Basis::eri_kernel,
+        src/integrals.rs:773-820): Rys for every quartet."""
+        with erf(omega):
+            return self.eri("rys")
 
     def eri(self, engine="auto"):
         n = self.nao
@@ -211,6 +218,21 @@ class OracleBasis:
         if rc != 0:
             raise RuntimeError(lib().orc_last_error().decode())
         return out.reshape(self.natom, 3), cnt.value, hsh.value
+
+
+class erf:
+    """Context: the oracle's Rys evaluations use erf(omega r)/r inside."""
+
+    def __init__(self, omega):
+        self.omega = float(omega)
+
+    def __enter__(self):
+        lib().orc_set_erf_omega(self.omega)
+        return self
+
+    def __exit__(self, *exc):
+        lib().orc_set_erf_omega(0.0)
+        return False
 
 
 def boys(m, t, reference=False):

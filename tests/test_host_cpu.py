@@ -73,6 +73,15 @@ def test_python_shell_validation_mirrors_reference():
     assert s.n_func() == 7 and s.n_cart() == 10
 
 
+def test_erf_kernel_requires_finite_positive_omega():
+    # tests/erf_kernel.rs:512-524: omega <= 0 (or not finite) is rejected
+    for bad in (0.0, -0.5, float("nan"), float("inf")):
+        with pytest.raises(ib.IntegralError):
+            ib.EriKernel.Erf(bad)
+    assert ib.EriKernel.Erf(0.4).omega == 0.4
+    assert ib.EriKernel.Coulomb.omega == 0.0
+
+
 def test_basis_metadata_without_device():
     shells = [ib.Shell.from_dict(d) for d in S.direct_grad_fixture(False)]
     B = ib.Basis(shells)

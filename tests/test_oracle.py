@@ -250,3 +250,76 @@ def test_gradient_single_atom_is_zero():
     coul, exch = S.grad_fixture_terms(B.nao)
     g, cnt, _ = B.direct_grad(coul, exch, 0.0)
     assert cnt == 0 and float(np.max(np.abs(g))) == 0.0
+
+
+# ------------------------------------------------------ erf attenuation
+
+def test_erf_ss_quartet_is_the_attenuated_boys_formula():
+    """(ss|ss) of erf(omega r)/r for single primitives equals
+    2 pi^(5/2)/(p q sqrt(p+q)) K_ab K_cd sqrt(s) F_0(s T), s = omega^2/(rho+omega^2)
+    (the root/weight transform of crates/integral/src/engine/rys.rs:163-175)."""
+    A, Bc, C, D = [0.0, 0.0, 0.0], [0.3, -0.2, 0.5], [1.1, 0.4, -0.6], [0.9, 1.2, 0.1]
+    ex = [1.3, 0.7, 0.9, 0.45]
+    shells = [dict(l=0, spherical=False, center=c, exps=[e], coefs=[1.0]) for c, e in zip((A, Bc, C, D), ex)]
+    OB = O.OracleBasis(shells)
+    omega = 0.4
+    with O.erf(omega):
+        got = OB.eri_block(0, 1, 2, 3, "rys").reshape(-1)[0]
+    a, b, c, d = ex
+    p, q = a + b, c + d
+    P = (a * np.array(A) + b * np.array(Bc)) / p
+    Q = (c * np.array(C) + d * np.array(D)) / q
+    kab = np.exp(-a * b / p * np.sum((np.array(A) - np.array(Bc)) ** 2))
+    kcd = np.exp(-c * d / q * np.sum((np.array(C) - np.array(D)) ** 2))
+    rho = p * q / (p + q)
+    T = rho * np.sum((P - Q) ** 2)
+    s = omega ** 2 / (rho + omega ** 2)
+    norm = np.prod([(2 * e / np.pi) ** 0.75 for e in ex])
+    want = 2 * np.pi ** 2.5 / (p * q * np.sqrt(p + q)) * kab * kcd * np.sqrt(s) * O.boys(0, s * T)[0] * norm
+    assert abs(got - want) < 1e-13 * abs(want)
+
+
+def test_erf_at_large_omega_is_coulomb():
+    shells = S.direct_contractor_fixture(False)
+    OB = O.OracleBasis(shells)
+    coul = OB.eri("rys")
+    att = OB.eri_erf(1e9)
+    assert float(np.max(np.abs(att - coul))) < 1e-12 * float(np.max(np.abs(coul)))
+    # and smaller omega attenuates: |erf| < |Coulomb| on the diagonal
+    att2 = OB.eri_erf(0.3)
+    n = OB.nao
+    dc, da = coul.reshape(n, n, n, n), att2.reshape(n, n, n, n)
+    diag_c = np.array([dc[i, j, i, j] for i in range(n) for j in range(n)])
+    diag_a = np.array([da[i, j, i, j] for i in range(n) for j in range(n)])
+    assert np.all(diag_a < diag_c)
+
+
+def test_erf_gradient_matches_finite_difference():
+    # tests/erf_gradients.rs:132-146: the attenuated gradient against central
+    # differences of the attenuated energy, omega in {0.3, 1.0}
+    shells = S.direct_grad_fixture(False)
+    B = O.OracleBasis(shells)
+    n = B.nao
+    coul, exch = S.grad_fixture_terms(n)
+    atoms = []
+    for s in shells:
+        if s["center"] not in atoms:
+            atoms.append(s["center"])
+    h = 2e-4
+    for omega in (0.3, 1.0):
+        with O.erf(omega):
+            g, _, _ = B.direct_grad(coul, exch, 0.0, engine="rys")
+        g0, _, _ = B.direct_grad(coul, exch, 0.0, engine="rys")
+        assert float(np.max(np.abs(g - g0))) > 1e-3 * float(np.max(np.abs(g0)))
+        assert float(np.max(np.abs(g.sum(axis=0)))) < 1e-10
+        for a, x in ((0, 0), (1, 2), (2, 1)):
+            vals = []
+            for sgn in (+1, -1):
+                moved = [dict(s, center=[c + (sgn * h if (s["center"] == atoms[a] and k == x) else 0.0)
+                                         for k, c in enumerate(s["center"])]) for s in shells]
+                E = O.OracleBasis(moved).eri_erf(omega).reshape(n, n, n, n)
+                e = sum(f * np.einsum("pq,pqrs,rs->", L, E, R) for f, L, R in coul)
+                e += sum(f * np.einsum("pr,pqrs,qs->", L, E, R) for f, L, R in exch)
+                vals.append(e)
+            fd = (vals[0] - vals[1]) / (2 * h)
+            assert abs(fd - g[a, x]) < 1e-6, (omega, a, x, fd, g[a, x])
