@@ -157,6 +157,31 @@ int igpu_eri_builder_fill(igpu_plan* plan, const uint32_t* bra_subset, size_t ns
  * Q_ij*Q_kl < threshold; threshold <= 0 screens nothing. */
 int igpu_eri_packed(igpu_plan* plan, double threshold, const uint32_t* bra_subset, size_t nsub, double* out);
 
+/* Density fitting (src/df.rs).  An auxiliary basis is attached to a plan
+ * (Eri3cBuilder::new(main, aux), df.rs:354-383); each aux shell is paired
+ * with the unit s dummy (one zero-exponent primitive of coefficient 1,
+ * df.rs:33-38), so (mu nu|P) = (mu nu|P 1s) and (P|Q) = (P 1s|Q 1s) run on the
+ * four-centre kernels.  Attaching again replaces the earlier aux basis; the
+ * main-basis entries are unaffected.  Aux shells are validated like main
+ * shells; l above the compiled GPU classes is IGPU_ERR_UNSUPPORTED.  The
+ * aux Schwarz factors are evaluated on the device here. */
+int igpu_plan_attach_aux(igpu_plan* plan, const igpu_shell* aux, size_t naux_shells);
+/* naux (aux functions) and the aux shell count of the attached basis. */
+int igpu_aux_query(const igpu_plan* plan, size_t* naux, size_t* naux_shells);
+/* Basis::schwarz_aux_bounds (df.rs:250-286): QP[p] = sqrt(max_mu (mu|mu))
+ * over the (p|p) block, one per aux shell. */
+int igpu_schwarz_aux(const igpu_plan* plan, double* qp);
+/* Basis::eri_2c / eri_2c_kernel (df.rs:49-145) over the attached aux basis:
+ * row-major naux x naux, exactly symmetric. */
+int igpu_eri_2c(igpu_plan* plan, double* out);
+/* Eri3cBuilder::build / fill / fill_filtered (df.rs:463-520): (mu nu|P) at
+ * out[(mu*nao + nu)*naux + P] for the canonical main bra pairs in bra_subset
+ * (all when NULL), both the (i, j) and (j, i) bands, over the aux shells p
+ * with keep[p] != 0 (all when keep is NULL).  `out` is the host buffer of
+ * nao*nao*naux doubles; slots of other bras and of skipped aux shells keep
+ * their content. */
+int igpu_eri_3c(igpu_plan* plan, const uint32_t* bra_subset, size_t nsub, const uint8_t* keep, double* out);
+
 /* DirectContractor::density_shell_bounds (direct.rs:103-125): per density the
  * max |D| of every ordered shell block, ndens x nsh x nsh. */
 int igpu_density_shell_bounds(const igpu_plan* plan, const double* dens, int ndens, double* bounds);

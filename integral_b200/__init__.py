@@ -158,14 +158,13 @@ class _Plan:
         """Operator of later calls: 0 Coulomb, > 0 erf(omega r)/r."""
         _lib.check(_lib.lib().igpu_set_erf_omega(self.h, float(omega)))
 
-    def __init__(self, shells: Sequence[Shell], engine: Engine):
-        L = _lib.lib()
+    @staticmethod
+    def _shell_array(shells: Sequence[Shell], keep: list):
         arr = (IgpuShell * max(1, len(shells)))()
-        self._keep = []
         for k, s in enumerate(shells):
             ex = np.ascontiguousarray(s._exps, dtype=np.float64)
             co = np.ascontiguousarray(s._coefs, dtype=np.float64)
-            self._keep += [ex, co]
+            keep += [ex, co]
             arr[k].l = s._l
             arr[k].spherical = 1 if s._kind == ShellKind.Spherical else 0
             for c in range(3):
@@ -173,6 +172,24 @@ class _Plan:
             arr[k].nprim = len(s._exps)
             arr[k].exps = ex.ctypes.data_as(c_double_p)
             arr[k].coefs = co.ctypes.data_as(c_double_p)
+        return arr
+
+    def attach_aux(self, aux: "Basis"):
+        """Attach `aux` as the density-fitting basis (once per aux object)."""
+        if getattr(self, "_aux", None) is aux:
+            return
+        keep = []
+        arr = self._shell_array(aux._shells, keep)
+        self._aux = None
+        _lib.check(_lib.lib().igpu_plan_attach_aux(self.h, arr, len(aux._shells)))
+        naux, nsh = ctypes.c_size_t(), ctypes.c_size_t()
+        _lib.check(_lib.lib().igpu_aux_query(self.h, ctypes.byref(naux), ctypes.byref(nsh)))
+        self._aux, self.naux, self.naux_sh = aux, naux.value, nsh.value
+
+    def __init__(self, shells: Sequence[Shell], engine: Engine):
+        L = _lib.lib()
+        self._keep = []
+        arr = self._shell_array(shells, self._keep)
         h = ctypes.c_void_p()
         _lib.check(L.igpu_plan_create(arr, len(shells), int(engine), ctypes.byref(h)))
         self.h = h
@@ -282,6 +299,74 @@ class Basis:
     def packed_eri_builder(self) -> "PackedEriBuilder":
         return PackedEriBuilder(self)
 
+    # --- density fitting over this basis as the auxiliary basis (src/df.rs)
+    def _aux_plan(self, engine: Engine) -> _Plan:
+        p = self.plan(engine)
+        p.attach_aux(self)
+        return p
+
+    def eri_2c(self) -> np.ndarray:
+        """Basis::eri_2c (src/df.rs:49-51): the metric (P|Q), row-major
+        naux x naux, exactly symmetric."""
+        return self.eri_2c_with(Engine.Auto)
+
+    def eri_2c_with(self, engine: Engine) -> np.ndarray:
+        p = self._aux_plan(engine)
+        out = np.empty(p.naux * p.naux)
+        _lib.check(_lib.lib().igpu_eri_2c(p.h, out.ctypes.data_as(c_double_p)))
+        return out
+
+    def eri_2c_kernel(self, kernel: "EriKernel") -> np.ndarray:
+        """Basis::eri_2c_kernel (src/df.rs:100-145)."""
+        p = self._aux_plan(Engine.Auto)
+        p.set_erf_omega(_omega_of(kernel))
+        try:
+            out = np.empty(p.naux * p.naux)
+            _lib.check(_lib.lib().igpu_eri_2c(p.h, out.ctypes.data_as(c_double_p)))
+        finally:
+            p.set_erf_omega(0.0)
+        return out
+
+    def schwarz_aux_bounds(self) -> np.ndarray:
+        """Basis::schwarz_aux_bounds (src/df.rs:250-286): one factor per shell."""
+        return self.schwarz_aux_bounds_with(Engine.Auto)
+
+    def schwarz_aux_bounds_with(self, engine: Engine) -> np.ndarray:
+        p = self._aux_plan(engine)
+        out = np.empty(p.naux_sh)
+        _lib.check(_lib.lib().igpu_schwarz_aux(p.h, out.ctypes.data_as(c_double_p)))
+        return out
+
+    def eri_3c_block(self, aux: "Basis", ish: int, jsh: int, psh: int) -> np.ndarray:
+        """Basis::eri_3c_block (src/df.rs:148-150): (ij|P) row-major
+        [n_i, n_j, n_p], P fastest."""
+        return self.eri_3c_block_with(Engine.Auto, aux, ish, jsh, psh)
+
+    def eri_3c_block_with(self, engine: Engine, aux: "Basis", ish: int, jsh: int, psh: int,
+                          kernel: "EriKernel" = None) -> np.ndarray:
+        nsh, nash = len(self._shells), len(aux._shells)
+        if not (0 <= ish < nsh and 0 <= jsh < nsh and 0 <= psh < nash):
+            raise IntegralError(-1, "invalid argument", "shell index out of range")
+        b = Eri3cBuilder(self, aux, engine)
+        i, j = max(ish, jsh), min(ish, jsh)
+        out = np.zeros(b.output_len())
+        keep = np.zeros(nash, dtype=np.uint8)
+        keep[psh] = 1
+        b._run(np.array([i * (i + 1) // 2 + j], dtype=np.uint32), keep, out, kernel)
+        n, naux = self.nao(), aux.nao()
+        oi, oj, op = self.offsets()[ish], self.offsets()[jsh], aux.offsets()[psh]
+        ni, nj, np_ = self._shells[ish].n_func(), self._shells[jsh].n_func(), aux._shells[psh].n_func()
+        T = out.reshape(n, n, naux)
+        return np.ascontiguousarray(T[oi:oi + ni, oj:oj + nj, op:op + np_]).reshape(-1)
+
+    def eri_3c_block_kernel(self, aux: "Basis", ish: int, jsh: int, psh: int, kernel: "EriKernel") -> np.ndarray:
+        """Basis::eri_3c_block_kernel (src/df.rs:201-246)."""
+        return self.eri_3c_block_with(Engine.Auto, aux, ish, jsh, psh, kernel)
+
+    def eri_3c_builder(self, aux: "Basis") -> "Eri3cBuilder":
+        """Basis::eri_3c_builder (src/df.rs:288-290)."""
+        return Eri3cBuilder(self, aux)
+
 
 # ------------------------------------------------------------ EriBuilder
 
@@ -347,6 +432,87 @@ class EriBuilder:
     def build(self) -> np.ndarray:
         out = np.zeros(self.output_len())
         self._run(None, 0, out)
+        return out
+
+
+# ------------------------------------------------------ density fitting
+
+@dataclass
+class Bra3cFill:
+    """One task of Eri3cBuilder.partition (src/df.rs:531-547): the canonical
+    main bra pair (i, j) and the output buffer whose (i, j) and (j, i) row
+    bands it fills."""
+    bra: tuple
+    index: int
+    out: np.ndarray
+
+
+class Eri3cBuilder:
+    """The dense 3-centre tensor (mu nu|P), row-major [nao, nao, naux] with P
+    fastest, over canonical main bra pairs (src/df.rs:325-520).  Each aux
+    shell is evaluated with the unit s dummy (df.rs:33-38)."""
+
+    def __init__(self, main: Basis, aux: Basis, engine: Engine = Engine.Auto):
+        self._main, self._aux = main, aux
+        self._plan = main.plan(engine)
+        self._pairs = self._plan.bra_pairs()
+        self._naux = aux.nao()
+
+    @classmethod
+    def new(cls, main: Basis, aux: Basis) -> "Eri3cBuilder":
+        return cls(main, aux)
+
+    @classmethod
+    def with_engine(cls, main: Basis, aux: Basis, engine: Engine) -> "Eri3cBuilder":
+        return cls(main, aux, engine)
+
+    def bra_pairs(self):
+        return list(self._pairs)
+
+    def output_len(self) -> int:
+        return self._plan.nao * self._plan.nao * self._naux
+
+    def partition(self, out: np.ndarray):
+        if out.size != self.output_len():
+            raise IntegralError(-7, "length mismatch", "3c output buffer must be nao^2*naux = %d elements"
+                                % self.output_len())
+        return [Bra3cFill(bra, k, out) for k, bra in enumerate(self._pairs)]
+
+    def _run(self, idx, keep, out, kernel=None):
+        if not out.flags["C_CONTIGUOUS"] or out.dtype != np.float64 or out.size != self.output_len():
+            raise IntegralError(-7, "length mismatch", "output must be contiguous float64 of nao^2*naux")
+        p = self._plan
+        p.attach_aux(self._aux)
+        p.set_erf_omega(_omega_of(kernel))
+        try:
+            _lib.check(_lib.lib().igpu_eri_3c(
+                p.h, idx.ctypes.data_as(c_u32_p) if idx is not None else None, 0 if idx is None else len(idx),
+                keep.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if keep is not None else None,
+                out.ctypes.data_as(c_double_p)))
+        finally:
+            p.set_erf_omega(0.0)
+
+    def fill(self, task: Bra3cFill):
+        """Eri3cBuilder::fill (src/df.rs:463-465)."""
+        self.fill_many([task])
+
+    def fill_filtered(self, task: Bra3cFill, keep):
+        """Eri3cBuilder::fill_filtered (src/df.rs:475-513): only the aux
+        shells p with keep(p) true; the others' slots are left untouched."""
+        mask = np.array([1 if keep(p) else 0 for p in range(len(self._aux._shells))], dtype=np.uint8)
+        self._run(np.array([task.index], dtype=np.uint32), mask, task.out)
+
+    def fill_many(self, tasks: Sequence[Bra3cFill]):
+        """Fill several tasks sharing one output buffer in one launch sequence."""
+        if not tasks:
+            return
+        idx = np.ascontiguousarray([t.index for t in tasks], dtype=np.uint32)
+        self._run(idx, None, tasks[0].out)
+
+    def build(self) -> np.ndarray:
+        """Eri3cBuilder::build (src/df.rs:516-522)."""
+        out = np.zeros(self.output_len())
+        self._run(None, None, out)
         return out
 
 

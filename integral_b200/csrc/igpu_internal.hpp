@@ -40,7 +40,9 @@ struct PrimPairD {
 };
 
 // One canonical shell pair (i >= j in the reference's sense) with its
-// evaluation orientation.
+// evaluation orientation.  An auxiliary pair of density fitting (an aux shell
+// with the unit s dummy, src/df.rs:1-37) has i = the aux shell's position in
+// the aux basis, j = -1 and tri = -1.
 struct PairD {
   int a, b;       // evaluation orientation shells (l_a >= l_b)
   int i, j;       // canonical shells (i >= j)
@@ -95,6 +97,8 @@ enum Mode : int {
   MODE_BUILDER = 3,
   MODE_GRAD = 4,
   MODE_PACKED = 5,
+  MODE_DF3 = 6,  // density fitting (mu nu|P): main pair x (aux shell, unit s)
+  MODE_DF2 = 7,  // density fitting (P|Q): (aux shell, unit s) x (aux shell, unit s)
 };
 
 struct JKDev {
@@ -165,6 +169,9 @@ struct KernelArgs {
   size_t acc_offset;     // slot offset of the running bra-block J accumulators
   int kinds;             // 0 all shells Cartesian, 1 all spherical, 2 mixed
   double omega;          // 0: Coulomb 1/r; > 0: long-range erf(omega r)/r
+  int naux;              // MODE_DF3 / MODE_DF2: auxiliary functions
+  size_t dense_len;      // MODE_DF3 / MODE_DF2: doubles in `dense`
+  unsigned* store_fault; // MODE_DF3 / MODE_DF2: set when an index falls outside `dense`
 };
 
 }  // namespace igpu

@@ -637,6 +637,69 @@ __device__ __forceinline__ void consume_packed(const KernelArgs& A, const double
   }
 }
 
+// Store of the density-fitting writers: an index outside the output raises
+// the launch's fault flag instead of writing.
+__device__ __forceinline__ void df_store(const KernelArgs& A, size_t at, double v) {
+  if (at < A.dense_len)
+    A.dense[at] = v;
+  else
+    atomicOr(A.store_fault, 1u);
+}
+
+// Unpacks block position q of a row-major [dims0][dims1][dims2][dims3] block.
+__device__ __forceinline__ void block_index(int q, const int dims[4], int idx[4]) {
+  idx[3] = q % dims[3];
+  int r = q / dims[3];
+  idx[2] = r % dims[2];
+  r /= dims[2];
+  idx[1] = r % dims[1];
+  idx[0] = r / dims[1];
+}
+
+// Three-centre tensor (Eri3cBuilder::fill, src/df.rs:463-513): the block is
+// (main pair | aux shell, unit s), or (aux shell, unit s | main pair) when
+// the aux class is the larger one.  Element (mu nu|P) goes to
+// out[(mu*nao + nu)*naux + P] and, for two distinct main shells, to
+// (nu mu|P) as well: the (i, j) and (j, i) bands of the reference.
+__device__ __forceinline__ void consume_df3(const KernelArgs& A, const double* B, const int dims[4],
+                                            const int offs[4], const int sh[4], bool aux_is_bra, int lane,
+                                            int T) {
+  const int m0 = aux_is_bra ? 2 : 0, m1 = aux_is_bra ? 3 : 1, pp = aux_is_bra ? 0 : 2;
+  const bool same = sh[m0] == sh[m1];
+  const size_t n = (size_t)A.nao, na = (size_t)A.naux;
+  const int total = dims[0] * dims[1] * dims[2] * dims[3];
+  for (int q = lane; q < total; q += T) {
+    int idx[4];
+    block_index(q, dims, idx);
+    const size_t mu = (size_t)(offs[m0] + idx[m0]), nu = (size_t)(offs[m1] + idx[m1]);
+    const size_t P = (size_t)(offs[pp] + idx[pp]);
+    const double v = B[q];
+    df_store(A, (mu * n + nu) * na + P, v);
+    if (!same) df_store(A, (nu * n + mu) * na + P, v);
+  }
+}
+
+// Two-centre metric (Basis::eri_2c, src/df.rs:56-93): the block is
+// (aux shell P, unit s | aux shell Q, unit s); (P|Q) and (Q|P) receive the
+// same value.  On a diagonal shell block only the elements with bra index
+// >= ket index are taken, the values the reference's mirrored writes leave,
+// so the matrix is exactly symmetric.
+__device__ __forceinline__ void consume_df2(const KernelArgs& A, const double* B, const int dims[4],
+                                            const int offs[4], const int sh[4], int lane, int T) {
+  const bool same = sh[0] == sh[2];
+  const size_t na = (size_t)A.naux;
+  const int total = dims[0] * dims[1] * dims[2] * dims[3];
+  for (int q = lane; q < total; q += T) {
+    int idx[4];
+    block_index(q, dims, idx);
+    if (same && idx[2] > idx[0]) continue;
+    const size_t P = (size_t)(offs[0] + idx[0]), Q = (size_t)(offs[2] + idx[2]);
+    const double v = B[q];
+    df_store(A, P * na + Q, v);
+    df_store(A, Q * na + P, v);
+  }
+}
+
 // Schwarz: sqrt(max |(mu nu|mu nu)|) over the function-space diagonal of the
 // (ij|ij) block (src/integrals.rs:850-860).
 __device__ __forceinline__ void consume_schwarz(const KernelArgs& A, const double* B, const int dims[4],
@@ -689,6 +752,12 @@ __device__ __forceinline__ void post_quartet(const KernelArgs& A, const ClassDim
       break;
     case MODE_SCHWARZ:
       consume_schwarz(A, B, dims, pb_index, lane, T, tmask);
+      break;
+    case MODE_DF3:
+      consume_df3(A, B, dims, offs, shl, pb.j < 0, lane, T);
+      break;
+    case MODE_DF2:
+      consume_df2(A, B, dims, offs, shl, lane, T);
       break;
     default:
       break;

@@ -185,3 +185,41 @@ def grad_fixture_terms(n: int):
     exchange-type product terms over three symmetric matrices."""
     p, da, db = grad_symmetric(n, 1), grad_symmetric(n, 2), grad_symmetric(n, 3)
     return [(0.5, p, p), (0.3, da, db)], [(-0.5, da, da), (-0.2, db, p)]
+
+
+# --------------------------------------------------------- density fitting
+
+def df_fixture():
+    """The main and auxiliary bases of the reference's tests/df.rs:31-51:
+    main = contracted s, two p on one centre, spherical d; aux = s, p,
+    spherical d, contracted s on or near the same centres."""
+    main = [
+        dict(l=0, spherical=False, center=[0.0, 0.0, 0.0], exps=[1.4, 0.5], coefs=[0.6, 0.5]),
+        dict(l=1, spherical=False, center=[0.6, -0.3, 0.2], exps=[0.9], coefs=[1.0]),
+        dict(l=1, spherical=False, center=[0.6, -0.3, 0.2], exps=[0.4], coefs=[1.0]),
+        dict(l=2, spherical=True, center=[-0.4, 0.7, -0.1], exps=[1.1], coefs=[1.0]),
+    ]
+    aux = [
+        dict(l=0, spherical=False, center=[0.0, 0.0, 0.0], exps=[2.1], coefs=[1.0]),
+        dict(l=1, spherical=False, center=[0.6, -0.3, 0.2], exps=[1.3], coefs=[1.0]),
+        dict(l=2, spherical=True, center=[-0.4, 0.7, -0.1], exps=[0.8], coefs=[1.0]),
+        dict(l=0, spherical=False, center=[0.3, 0.1, -0.2], exps=[1.9, 0.7], coefs=[0.4, 0.8]),
+    ]
+    return main, aux
+
+
+def df_system(seed: int = 6, natom: int = 5, side: float = 7.0, spherical: bool = True):
+    """Density-fitting parity case: ``natom`` atoms in a ``side``-bohr cube
+    (min separation 1.5); main s,s,p,p,d,f of 3 primitives 0.12*2.5^k
+    (coefficients U(0.2,1.0)); aux s,p,d,f,s,p,d of single primitives
+    0.2*1.8^k scaled per shell by U(0.8,1.2), one kind for both bases."""
+    rng = np.random.default_rng(seed)
+    centers = place_atoms(rng, natom, side, 1.5)
+    main = build_shells(rng, centers, "ssppdf", 3, 0.12, 2.5, 0.2, 1.0, spherical=spherical)
+    aux = []
+    for c in centers:
+        for k, letter in enumerate("spdfspd"):
+            e = 0.2 * 1.8 ** k * rng.uniform(0.8, 1.2)
+            aux.append(dict(l=L_OF[letter], spherical=spherical, center=[float(x) for x in c],
+                            exps=[float(e)], coefs=[1.0]))
+    return dict(name="df_%datom" % natom, main=main, aux=aux, seed=seed)

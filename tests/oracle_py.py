@@ -277,3 +277,85 @@ def select_engine(ne, nf, deg):
     o = ctypes.c_int()
     lib().orc_select_engine(ne, nf, deg, ctypes.byref(o))
     return ["auto", "os", "rys"][o.value]
+
+
+# ------------------------------------------------------- density fitting
+
+def _nf(s):
+    return (2 * s["l"] + 1) if s.get("spherical") else (s["l"] + 1) * (s["l"] + 2) // 2
+
+
+def _offsets(shells):
+    out, acc = [], 0
+    for s in shells:
+        out.append(acc)
+        acc += _nf(s)
+    return out, acc
+
+
+def unit_s(center):
+    """The unit s dummy of src/df.rs:33-38: one zero-exponent primitive of
+    coefficient 1 (exempt from normalisation, src/shell.rs:182-187), the
+    constant function 1."""
+    return dict(l=0, spherical=False, center=list(center), exps=[0.0], coefs=[1.0])
+
+
+def df_eri_3c(main, aux, engine="auto", keep=None):
+    """Eri3cBuilder::build / fill_filtered (src/df.rs:463-522): for every
+    canonical main pair (i >= j) and aux shell p (with keep[p]), the block
+    (ij|p 1s) into the (i, j) band and, for i != j, the (j, i) band of the
+    row-major [nao, nao, naux] tensor, P fastest."""
+    nm, na = len(main), len(aux)
+    B = OracleBasis(list(main) + list(aux) + [unit_s(s["center"]) for s in aux])
+    mo, nao = _offsets(main)
+    ao, naux = _offsets(aux)
+    out = np.zeros((nao, nao, naux))
+    for i in range(nm):
+        for j in range(i + 1):
+            ni, nj = _nf(main[i]), _nf(main[j])
+            for p in range(na):
+                if keep is not None and not keep[p]:
+                    continue
+                blk = B.eri_block(i, j, nm + p, nm + na + p, engine)[..., 0]
+                sl = slice(ao[p], ao[p] + _nf(aux[p]))
+                out[mo[i]:mo[i] + ni, mo[j]:mo[j] + nj, sl] = blk
+                if i != j:
+                    out[mo[j]:mo[j] + nj, mo[i]:mo[i] + ni, sl] = blk.transpose(1, 0, 2)
+    return out.reshape(-1)
+
+
+def df_eri_3c_block(main, aux, ish, jsh, psh, engine="auto"):
+    """Basis::eri_3c_block_with (src/df.rs:155-185): (ij|p 1s), [n_i, n_j, n_p]."""
+    nm = len(main)
+    B = OracleBasis(list(main) + [aux[psh], unit_s(aux[psh]["center"])])
+    return B.eri_block(ish, jsh, nm, nm + 1, engine)[..., 0].reshape(-1)
+
+
+def df_eri_2c(aux, engine="auto"):
+    """Basis::eri_2c_with (src/df.rs:56-93): (p 1s|q 1s) for q <= p, written
+    to both orientations in the reference's element order, so a diagonal
+    shell block takes its lower-triangle values on both sides."""
+    na = len(aux)
+    B = OracleBasis(list(aux) + [unit_s(s["center"]) for s in aux])
+    ao, naux = _offsets(aux)
+    out = np.zeros((naux, naux))
+    for p in range(na):
+        for q in range(p + 1):
+            blk = B.eri_block(p, na + p, q, na + q, engine)[:, 0, :, 0]
+            for a in range(blk.shape[0]):
+                for b in range(blk.shape[1]):
+                    out[ao[p] + a, ao[q] + b] = blk[a, b]
+                    out[ao[q] + b, ao[p] + a] = blk[a, b]
+    return out.reshape(-1)
+
+
+def df_schwarz_aux(aux, engine="auto"):
+    """Basis::schwarz_aux_bounds_with (src/df.rs:257-286): sqrt of the
+    largest diagonal element of the (p 1s|p 1s) block, per aux shell."""
+    na = len(aux)
+    B = OracleBasis(list(aux) + [unit_s(s["center"]) for s in aux])
+    out = np.zeros(na)
+    for p in range(na):
+        blk = B.eri_block(p, na + p, p, na + p, engine)[:, 0, :, 0]
+        out[p] = np.sqrt(np.max(np.abs(np.diag(blk))))
+    return out

@@ -323,3 +323,115 @@ def test_erf_gradient_matches_finite_difference():
                 vals.append(e)
             fd = (vals[0] - vals[1]) / (2 * h)
             assert abs(fd - g[a, x]) < 1e-6, (omega, a, x, fd, g[a, x])
+
+
+# ------------------------------------------------------ density fitting
+# The oracle's restatement of src/df.rs pinned by the reference's own
+# tests/df.rs: closed forms, the zero-exponent limit, cross-engine agreement,
+# positive definiteness and the aux Schwarz bound.
+
+def _s_norm(a):
+    return (2.0 * a / np.pi) ** 0.75
+
+
+def _close(a, b, tol):
+    assert abs(a - b) / max(abs(b), 1.0) < tol, (a, b)
+
+
+def test_df_2c_concentric_s_closed_form():
+    # tests/df.rs:53-68
+    a, b = 0.9, 1.7
+    aux = [dict(l=0, spherical=False, center=[0.0] * 3, exps=[a], coefs=[1.0]),
+           dict(l=0, spherical=False, center=[0.0] * 3, exps=[b], coefs=[1.0])]
+    m = O.df_eri_2c(aux)
+    pref = lambda x, y: 2.0 * np.pi ** 2.5 / (x * y * np.sqrt(x + y))
+    _close(m[1], _s_norm(a) * _s_norm(b) * pref(a, b), 1e-12)
+    _close(m[0], _s_norm(a) ** 2 * pref(a, a), 1e-12)
+    _close(m[3], _s_norm(b) ** 2 * pref(b, b), 1e-12)
+    assert m[1] == m[2]
+
+
+def test_df_3c_concentric_s_closed_form():
+    # tests/df.rs:70-91
+    a, b, c = 0.8, 1.1, 0.6
+    main = [dict(l=0, spherical=False, center=[0.0] * 3, exps=[a], coefs=[1.0]),
+            dict(l=0, spherical=False, center=[0.0] * 3, exps=[b], coefs=[1.0])]
+    aux = [dict(l=0, spherical=False, center=[0.0] * 3, exps=[c], coefs=[1.0])]
+    blk = O.df_eri_3c_block(main, aux, 0, 1, 0)
+    p = a + b
+    want = _s_norm(a) * _s_norm(b) * _s_norm(c) * 2.0 * np.pi ** 2.5 / (p * c * np.sqrt(p + c))
+    assert blk.size == 1
+    _close(blk[0], want, 1e-12)
+
+
+def test_df_3c_matches_tiny_exponent_four_centre_limit():
+    # tests/df.rs:93-123: the dummy against an explicit s shell of exponent
+    # 1e-12 with effective coefficient 1
+    main, aux = S.df_fixture()
+    eps = 1e-12
+    nm = len(main)
+    for psh, sp in enumerate(aux):
+        tiny = dict(l=0, spherical=False, center=list(sp["center"]), exps=[eps], coefs=[1.0 / _s_norm(eps)])
+        four = O.OracleBasis(list(main) + [sp, tiny])
+        for ish in range(nm):
+            for jsh in range(nm):
+                got = O.df_eri_3c_block(main, aux, ish, jsh, psh)
+                want = four.eri_block(ish, jsh, nm, nm + 1).reshape(-1)
+                peak = float(np.max(np.abs(want)))
+                assert float(np.max(np.abs(got - want))) <= 1e-8 * peak + 1e-12
+
+
+def test_df_cross_engine_symmetry_and_definiteness():
+    # tests/df.rs:125-195
+    main, aux = S.df_fixture()
+    os_, rys = O.df_eri_2c(aux, "os"), O.df_eri_2c(aux, "rys")
+    peak = float(np.max(np.abs(os_)))
+    assert float(np.max(np.abs(os_ - rys))) <= 1e-11 * max(peak, 1.0)
+    m = O.df_eri_2c(aux)
+    n = int(round(np.sqrt(m.size)))
+    M = m.reshape(n, n)
+    assert np.array_equal(M, M.T) and np.all(np.diag(M) > 0.0)
+    np.linalg.cholesky(M)
+    for ish in range(len(main)):
+        for jsh in range(len(main)):
+            for psh in range(len(aux)):
+                a = O.df_eri_3c_block(main, aux, ish, jsh, psh, "os")
+                b = O.df_eri_3c_block(main, aux, ish, jsh, psh, "rys")
+                assert float(np.max(np.abs(a - b))) <= 1e-11 * max(float(np.max(np.abs(a))), 1.0)
+
+
+def test_df_schwarz_aux_bound_holds_for_all_3c_blocks():
+    # tests/df.rs:197-222
+    main, aux = S.df_fixture()
+    q = O.OracleBasis(main).schwarz()
+    qp = O.df_schwarz_aux(aux)
+    assert qp.shape == (len(aux),)
+    for ish in range(len(main)):
+        for jsh in range(len(main)):
+            for psh in range(len(aux)):
+                bound = q[ish, jsh] * qp[psh]
+                blk = O.df_eri_3c_block(main, aux, ish, jsh, psh)
+                assert float(np.max(np.abs(blk))) <= bound * (1.0 + 1e-10) + 1e-14
+
+
+def test_df_builder_equals_blockwise_assembly_and_erf_limit():
+    # tests/df.rs:224-266: the assembled tensor is the blocks in both bands;
+    # tests/erf_kernel.rs:428-481: erf at large omega is Coulomb
+    main, aux = S.df_fixture()
+    T = O.df_eri_3c(main, aux)
+    mo, nao = O._offsets(main)
+    ao, naux = O._offsets(aux)
+    T = T.reshape(nao, nao, naux)
+    for ish in range(len(main)):
+        for jsh in range(len(main)):
+            for psh in range(len(aux)):
+                ni, nj, npp = O._nf(main[ish]), O._nf(main[jsh]), O._nf(aux[psh])
+                blk = O.df_eri_3c_block(main, aux, ish, jsh, psh).reshape(ni, nj, npp)
+                got = T[mo[ish]:mo[ish] + ni, mo[jsh]:mo[jsh] + nj, ao[psh]:ao[psh] + npp]
+                assert float(np.max(np.abs(got - blk))) <= 1e-13 * max(float(np.max(np.abs(blk))), 1.0)
+    with O.erf(1e9):
+        T2 = O.df_eri_3c(main, aux, "rys").reshape(nao, nao, naux)
+        M2 = O.df_eri_2c(aux, "rys")
+    assert float(np.max(np.abs(T2 - T))) < 1e-12 * float(np.max(np.abs(T)))
+    M = O.df_eri_2c(aux)
+    assert float(np.max(np.abs(M2 - M))) < 1e-12 * float(np.max(np.abs(M)))
