@@ -59,6 +59,16 @@ def test_plan_create_validation_codes():
     assert b"NULL" in L.igpu_last_error_string()
 
 
+def test_density_fitting_entries_reject_null_arguments():
+    L = _lib.lib()
+    assert L.igpu_plan_attach_aux(None, None, 0) == -1
+    assert L.igpu_aux_query(None, None, None) == -1
+    assert L.igpu_schwarz_aux(None, None) == -1
+    assert L.igpu_eri_2c(None, None) == -1
+    assert L.igpu_eri_3c(None, None, 0, None, None) == -1
+    assert b"NULL" in L.igpu_last_error_string()
+
+
 def test_python_shell_validation_mirrors_reference():
     with pytest.raises(ib.IntegralError) as e:
         ib.Shell(0, [0, 0, 0], [], [])
@@ -148,6 +158,50 @@ def test_two_rank_sharded_jk_equals_single_rank(tmp_path):
     assert int(r["count"][0]) == cnt
     assert float(np.max(np.abs(r["J"] - J))) < 1e-12 * float(np.max(np.abs(J)))
     assert float(np.max(np.abs(r["K"] - K))) < 1e-12 * float(np.max(np.abs(K)))
+
+
+def _grad_rank_main(rank, world, port, result_path):
+    import sys
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import torch.distributed as dist
+    import oracle_py as O
+    from integral_b200 import sharding as sh
+    from integral_b200 import systems as syst
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world)
+    shells = syst.direct_grad_fixture(False)
+    B = O.OracleBasis(shells)
+    coul, exch = syst.grad_fixture_terms(B.nao)
+    nbra = len(shells) * (len(shells) + 1) // 2
+    g, cnt, _ = B.direct_grad(coul, exch, 1e-10, bras=sh.bra_shard(nbra, rank, world))
+    counts = np.array([float(cnt)])
+    sh.all_reduce_sum([g, counts])
+    if rank == 0:
+        np.savez(result_path, g=g, count=counts)
+    dist.destroy_process_group()
+
+
+def test_two_rank_sharded_gradient_equals_single_rank(tmp_path):
+    """World size 2 over gloo: each rank contracts the gradient of its bra
+    shard (DirectGradContractor::accumulate_bra_pair over its pairs); one
+    all-reduce of the natom x 3 forces gives the unsharded contraction."""
+    import socket
+
+    import torch.multiprocessing as mp
+    sock = socket.socket()
+    sock.bind(("127.0.0.1", 0))
+    port = sock.getsockname()[1]
+    sock.close()
+    out = str(tmp_path / "g.npz")
+    mp.start_processes(_grad_rank_main, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
+    import oracle_py as O
+    shells = S.direct_grad_fixture(False)
+    B = O.OracleBasis(shells)
+    coul, exch = S.grad_fixture_terms(B.nao)
+    g, cnt, _ = B.direct_grad(coul, exch, 1e-10)
+    r = np.load(out)
+    assert int(r["count"][0]) == cnt
+    assert float(np.max(np.abs(r["g"] - g))) < 1e-12 * float(np.max(np.abs(g)))
 
 
 def test_bench_reference_arm_prints_the_contract_line():
