@@ -180,6 +180,18 @@ int orc_direct_grad(void* g, int ncoul, const double* cf, const double* cl, cons
   }
 }
 
+// Dense-gamma gradient (Basis::eri_grad_contract_with); out is natom x 3
+// and accumulates.
+int orc_eri_grad_contract(void* g, const double* gamma, double* out) {
+  try {
+    static_cast<GradHandle*>(g)->plan.dense_contract(gamma, out);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
 void orc_boys(int m, double t, double* out) { boys_array(m, t, out); }
 void orc_boys_reference(int m, double t, double* out) { boys_reference(m, t, out); }
 void orc_rys(int n, double t, double* r, double* w) { rys_roots_weights(n, t, r, w); }

@@ -331,8 +331,15 @@ void GradPlan::shifted_block(const int idx[4], int pos, int lp, bool weighted, b
 // direct_grad.rs:394-485
 void GradPlan::quartet(const int idx[4], double degeneracy, const GradDensity& dens,
                        double* out) const {
+  contract_weights(idx, weight_block(idx, degeneracy, dens), out);
+}
+
+// The derivative of one shell quartet contracted with its Cartesian weight
+// block w: raised (2-alpha weighted) and lowered blocks on positions 0..2,
+// the fourth centre by translational invariance (direct_grad.rs:431-485).
+void GradPlan::contract_weights(const int idx[4], const std::vector<double>& w,
+                                double* out) const {
   const auto& sh = basis.shells();
-  std::vector<double> w = weight_block(idx, degeneracy, dens);
   int ls[4], dims[4];
   for (int p = 0; p < 4; ++p) {
     ls[p] = sh[idx[p]].l;
@@ -393,6 +400,41 @@ void GradPlan::quartet(const int idx[4], double degeneracy, const GradDensity& d
   }
   int atom = basis.shell_atom()[idx[3]];
   for (int axis = 0; axis < 3; ++axis) out[(size_t)atom * 3 + axis] += fourth[axis];
+}
+
+// Basis::eri_grad_contract_with (grad.rs:427-470): the gradient of
+// E = sum over all ordered quartets of gamma[mu nu la si] (mu nu|la si), the
+// reference's dense oracle of the direct gradient.  gamma is nao^4, function
+// space.  Each ordered quartet is evaluated in the orientation with i >= j
+// and k >= l (the pair data are stored for canonical pairs), its gamma block
+// permuted to match; the derivative of a permuted block is the permuted
+// derivative, so the contraction is unchanged.
+void GradPlan::dense_contract(const double* gamma, double* out) const {
+  const auto& sh = basis.shells();
+  const auto& offs = basis.offsets();
+  const size_t n = (size_t)basis.nao();
+  const int nsh = basis.nsh();
+  for (int i = 0; i < nsh; ++i)
+    for (int j = 0; j < nsh; ++j)
+      for (int k = 0; k < nsh; ++k)
+        for (int l = 0; l < nsh; ++l) {
+          const bool sb = i < j, sk = k < l;
+          const int idx[4] = {sb ? j : i, sb ? i : j, sk ? l : k, sk ? k : l};
+          int dims[4];
+          for (int p = 0; p < 4; ++p) dims[p] = sh[idx[p]].n_func();
+          std::vector<double> w((size_t)dims[0] * dims[1] * dims[2] * dims[3]);
+          const int ni = sh[i].n_func(), nj = sh[j].n_func(), nk = sh[k].n_func(), nl = sh[l].n_func();
+          for (int a = 0; a < ni; ++a)
+            for (int b = 0; b < nj; ++b)
+              for (int c = 0; c < nk; ++c)
+                for (int d = 0; d < nl; ++d) {
+                  const int x0 = sb ? b : a, x1 = sb ? a : b, x2 = sk ? d : c, x3 = sk ? c : d;
+                  w[(((size_t)x0 * dims[1] + x1) * dims[2] + x2) * dims[3] + x3] =
+                      gamma[(((size_t)(offs[i] + a) * n + offs[j] + b) * n + offs[k] + c) * n + offs[l] + d];
+                }
+          const std::vector<double>* mats[4] = {&s2c[idx[0]], &s2c[idx[1]], &s2c[idx[2]], &s2c[idx[3]]};
+          contract_weights(idx, transform_block4(std::move(w), dims, mats), out);
+        }
 }
 
 // direct_grad.rs:328-373

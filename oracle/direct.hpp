@@ -77,6 +77,8 @@ struct GradPlan {
   void shifted_block(const int idx[4], int pos, int lp, bool weighted, bool use_rys,
                      double* out) const;
   void quartet(const int idx[4], double degeneracy, const GradDensity& d, double* out) const;
+  void contract_weights(const int idx[4], const std::vector<double>& w, double* out) const;
+  void dense_contract(const double* gamma, double* out) const;
   void accumulate_bra_pair(int i, int j, const GradDensity& d, double threshold, double* out,
                            QuartetSink* sink, bool count_only) const;
 };

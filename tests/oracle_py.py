@@ -66,6 +66,7 @@ def lib():
                                       ctypes.c_int, c_double_p, c_double_p, c_double_p, ctypes.c_double,
                                       c_int_p, ctypes.c_int, ctypes.c_int, c_double_p, c_u64_p, c_u64_p,
                                       ctypes.c_int]
+        L.orc_eri_grad_contract.argtypes = [ctypes.c_void_p, c_double_p, c_double_p]
         L.orc_boys.argtypes = [ctypes.c_int, ctypes.c_double, c_double_p]
         L.orc_boys_reference.argtypes = [ctypes.c_int, ctypes.c_double, c_double_p]
         L.orc_rys.argtypes = [ctypes.c_int, ctypes.c_double, c_double_p, c_double_p]
@@ -218,6 +219,17 @@ class OracleBasis:
         if rc != 0:
             raise RuntimeError(lib().orc_last_error().decode())
         return out.reshape(self.natom, 3), cnt.value, hsh.value
+
+    def eri_grad_contract(self, gamma, engine="auto"):
+        """Basis::eri_grad_contract_with (src/grad.rs:427-470): the gradient of
+        sum gamma[p,q,r,s] (pq|rs) over all ordered quartets; gamma nao^4."""
+        g = np.ascontiguousarray(gamma, dtype=np.float64).reshape(-1)
+        if g.size != self.nao ** 4:
+            raise ValueError("gamma must have nao^4 elements")
+        out = np.zeros(self.natom * 3)
+        if lib().orc_eri_grad_contract(self._gplan(engine), _dp(g), _dp(out)) != 0:
+            raise RuntimeError(lib().orc_last_error().decode())
+        return out.reshape(self.natom, 3)
 
 
 class erf:

@@ -435,3 +435,34 @@ def test_df_builder_equals_blockwise_assembly_and_erf_limit():
     assert float(np.max(np.abs(T2 - T))) < 1e-12 * float(np.max(np.abs(T)))
     M = O.df_eri_2c(aux)
     assert float(np.max(np.abs(M2 - M))) < 1e-12 * float(np.max(np.abs(M)))
+
+
+
+# ------------------------------------------------- dense-gamma gradient
+
+def _dense_gamma(n, coulomb, exchange):
+    """tests/direct_grad_contractor.rs:106-129."""
+    G = np.zeros((n, n, n, n))
+    for f, L, R in coulomb:
+        G += f * np.einsum("pq,rs->pqrs", L, R)
+    for f, L, R in exchange:
+        G += f * np.einsum("pr,qs->pqrs", L, R)
+    return G
+
+
+@pytest.mark.parametrize("spherical,engine,omega", [(False, "os", 0.0), (True, "os", 0.0), (False, "rys", 0.0),
+                                                    (True, "auto", 0.0), (True, "rys", 0.3), (False, "rys", 1.7)])
+def test_direct_gradient_matches_dense_gamma_contraction(spherical, engine, omega):
+    # tests/direct_grad_contractor.rs:157-225: the density-direct contraction
+    # equals eri_grad_contract of the dense gamma within 1e-10, zero net force
+    shells = S.direct_grad_fixture(spherical)
+    B = O.OracleBasis(shells)
+    n = B.nao
+    coul, exch = S.grad_fixture_terms(n)
+    gamma = _dense_gamma(n, coul, exch)
+    with O.erf(omega):
+        ref = B.eri_grad_contract(gamma, engine)
+        g, _, _ = B.direct_grad(coul, exch, 0.0, engine=engine)
+    assert float(np.max(np.abs(g - ref))) < 1e-10
+    assert float(np.max(np.abs(g.sum(axis=0)))) < 1e-10
+    assert float(np.max(np.abs(g))) > 1e-3
