@@ -57,9 +57,10 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-sample-bras", type=int, default=24)
-    p.add_argument("--workload", default="jk", choices=["jk", "grad"],
+    p.add_argument("--workload", default="jk", choices=["jk", "grad", "dense"],
                    help="jk: the headline J/K build (default); grad: the density-direct ERI gradient of the "
-                        "100-atom / nao 1400 system on an interleaved 1/--grad-stride share of the bra pairs")
+                        "100-atom / nao 1400 system on an interleaved 1/--grad-stride share of the bra pairs; "
+                        "dense: the dense nao^4 tensor of the 6-atom / nao 54 system")
     # a stride > 1 still decodes every task (the subset is a filter), so its
     # quartets/s understates the full build's
     p.add_argument("--grad-stride", type=int, default=1)
@@ -125,6 +126,89 @@ def grad_bench(args):
         "max_abs_mixed_minus_fp64": float(np.abs(g32 - g64).max()),
         "max_abs_gradient": float(np.abs(g64).max()),
         "e2e": {"value": q32 / w32, "unit": "quartets/s"},
+    }
+    print(json.dumps(line))
+
+
+def dense_bench(args):
+    """Dense ERI tensor (Basis::eri) of the 6-atom, nao 54 Cartesian
+    s,s,s,p,p system: 108 345 canonical quartets of 81 primitive quartets,
+    every one scattered to its distinct permutation slots of the 54^4 FP64
+    tensor (68 MB).  value = canonical quartets per second of kernel time
+    (CUDA events around every launch on the plan's stream); L2 flushed
+    before each step (a 256 MB write), since the output fits in L2.  The
+    roofline is the HBM write of the tensor; e2e is the C-ABI call with the
+    zero fill and the D2H of the tensor."""
+    import torch
+
+    torch.cuda.set_device(0)
+    import integral_b200 as ib
+    from integral_b200 import systems as S
+
+    s = S.dense_eri_system()
+    B = ib.Basis(s["shells"])
+    p = B.plan()
+    n = p.nao
+    out = np.empty(n ** 4)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    lib = ib._lib.lib()
+
+    def step():
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        ib._lib.check(lib.igpu_eri_dense(p.h, out.ctypes.data_as(ib._lib.c_double_p)))
+        return time.perf_counter() - t, p.stats()
+
+    for _ in range(args.warmup):
+        step()
+    clk = ClockSampler(0)
+    clk.start()
+    wall, ms, q, launches = 0.0, 0.0, 0, 0
+    for _ in range(args.steps):
+        w, st = step()
+        wall += w
+        ms += st["kernel_ms"]
+        q += st["quartets"]
+        launches += st["launches"]
+    clocks = clk.stop()
+    prof = p.profile()
+    top = max(prof, key=lambda r: r["ms"])
+    tensor_bytes = 8.0 * n ** 4
+    achieved = tensor_bytes / (ms / args.steps * 1e-3) / 1e9
+    peak, peak_kind = None, "fallback"
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+            peak_kind = "measured"
+    except (OSError, KeyError, ValueError):
+        peak = 6650.0
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_py as O
+    ob = O.OracleBasis(s["shells"])
+    t0 = time.perf_counter()
+    ob.eri()
+    cpu_s = time.perf_counter() - t0
+    nq = q // args.steps
+    line = {
+        "metric": "dense ERI tensor canonical quartets/s on B200", "unit": "quartets/s",
+        "value": q / (ms * 1e-3), "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded generator, no data set)",
+        "config": {"workload": "dense ERI tensor, 6 atoms in 8-bohr cube, s,s,s,p,p Cartesian, 3 primitives, "
+                               "nao 54, 54^4 FP64 output", "quartets_per_step": nq,
+                   "l2": "flushed before every step (256 MB write)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "note": "algorithmic bytes = the 68 MB tensor written once per step, over the summed "
+                             "device time of the step's launches (%s peak)" % peak_kind},
+        "top_launch": {"class": "(%d%d|%d%d)" % (top["la"], top["lb"], top["lc"], top["ld"]), "ms": top["ms"]},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "e2e": {"value": nq * args.steps / wall, "unit": "quartets/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(tensor_bytes)},
+        "cpu_baseline": {"value": nq / cpu_s, "unit": "quartets/s", "cores": 1, "kind": "port",
+                         "sample": "the whole tensor once, C++ restatement of Basis::eri"},
     }
     print(json.dumps(line))
 
@@ -312,6 +396,8 @@ def main():
         return profile_case(args.workload)
     if args.workload == "grad":
         return grad_bench(args)
+    if args.workload == "dense":
+        return dense_bench(args)
     if args.impl == "reference":
         return reference_arm(args)
     import torch

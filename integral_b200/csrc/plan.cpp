@@ -1026,15 +1026,13 @@ static int dense_like(igpu_plan* P, bool builder, const uint32_t* sub, size_t ns
   KernelArgs A = base_args(P);
   A.mode = builder ? MODE_BUILDER : MODE_DENSE;
   A.dense = P->d_dense.p;
-  A.counters = nullptr;
   uint32_t launches = 0;
   rc = run_tasks(P, *ts, A, P->stream, launches);
   if (rc) return rc;
   CK(cudaMemcpyAsync(out, P->d_dense.p, n4 * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
   CK(cudaStreamSynchronize(P->stream));
-  P->last = igpu_stats{};
-  P->last.launches = launches;
-  return IGPU_OK;
+  // per-launch device times and quartet counts (igpu_last_stats / _profile)
+  return collect_profile(P, 0, false);
 }
 
 int igpu_eri_dense(igpu_plan* P, double* out) { return dense_like(P, false, nullptr, 0, out); }
