@@ -57,10 +57,13 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-sample-bras", type=int, default=24)
-    p.add_argument("--workload", default="jk", choices=["jk", "grad", "dense"],
+    p.add_argument("--workload", default="jk", choices=["jk", "grad", "dense", "jk-sph"],
                    help="jk: the headline J/K build (default); grad: the density-direct ERI gradient of the "
                         "100-atom / nao 1400 system on an interleaved 1/--grad-stride share of the bra pairs; "
-                        "dense: the dense nao^4 tensor of the 6-atom / nao 54 system")
+                        "dense: the dense nao^4 tensor of the 6-atom / nao 54 system; jk-sph: J/K of the "
+                        "200-atom / nao 5200 spherical system on an interleaved 1/--sph-stride share of the "
+                        "bra pairs")
+    p.add_argument("--sph-stride", type=int, default=512)
     # a stride > 1 still decodes every task (the subset is a filter), so its
     # quartets/s understates the full build's
     p.add_argument("--grad-stride", type=int, default=1)
@@ -209,6 +212,85 @@ def dense_bench(args):
                 "d2h_bytes_per_step": int(tensor_bytes)},
         "cpu_baseline": {"value": nq / cpu_s, "unit": "quartets/s", "cores": 1, "kind": "port",
                          "sample": "the whole tensor once, C++ restatement of Basis::eri"},
+    }
+    print(json.dumps(line))
+
+
+def jk_sph_bench(args):
+    """Direct J/K of the 200-atom, nao 5200 spherical s,s,s,p,p,d,d,f system
+    (4 primitives, 2 densities, tau 1e-11) on every --sph-stride-th canonical
+    bra pair: a full build takes hours on one GPU, and contributions are
+    additive per bra pair, so an interleaved share gives the rate and
+    stride x its time estimates the full build.  FP32-mixed and FP64, device
+    time (CUDA events on the launching stream), L2 flushed between steps."""
+    import torch
+
+    torch.cuda.set_device(0)
+    import integral_b200 as ib
+    from integral_b200 import systems as S
+
+    system = S.jk_spherical_system()
+    nd = system["dens"].shape[0]
+    thr = system["threshold"]
+    dc = ib.Basis(system["shells"]).direct_contractor()
+    nbra = len(dc.bra_pairs())
+    bras = np.arange(0, nbra, args.sph_stride, dtype=np.uint32)
+    D = torch.from_numpy(system["dens"]).cuda()
+    J, K = torch.zeros_like(D), torch.zeros_like(D)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def timed(prec, warm, steps):
+        for _ in range(warm):
+            J.zero_()
+            K.zero_()
+            dc.jk_device(D.data_ptr(), nd, J.data_ptr(), K.data_ptr(), thr, True, prec, bras=bras,
+                         stream=stream.cuda_stream)
+        ms, q, launches = 0.0, 0, 0
+        for _ in range(steps):
+            J.zero_()
+            K.zero_()
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            dc.jk_device(D.data_ptr(), nd, J.data_ptr(), K.data_ptr(), thr, True, prec, bras=bras,
+                         stream=stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            st = dc.last_stats()
+            q += st["quartets"]
+            launches += st["launches"] + 4
+        return ms, q, launches
+
+    clk = ClockSampler(0)
+    clk.start()
+    ms32, q32, l32 = timed(1, args.warmup, args.steps)
+    clocks = clk.stop()
+    Jm, Km = J.cpu().numpy().copy(), K.cpu().numpy().copy()
+    ms64, q64, _ = timed(0, 1, args.steps)
+    J64, K64 = J.cpu().numpy(), K.cpu().numpy()
+    Dn = system["dens"]
+    dE = sum(0.5 * float(np.sum(Dn[d] * ((Jm[d] - J64[d]) - 0.5 * (Km[d] - K64[d])))) for d in range(nd))
+    st = args.steps
+    line = {
+        "metric": "Fock J/K build quartets/s (FP32-mixed) on B200, spherical f, sampled bra pairs",
+        "unit": "quartets/s", "value": q32 / (ms32 * 1e-3), "n_gpus": 1, "steps": st, "warmup": args.warmup,
+        "ms_per_step": ms32 / st, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "fp32-mixed (fp64 accumulation)", "data": "synthetic (seeded generator, no data set)",
+        "config": {"workload": "direct J/K, 200 atoms in 32-bohr cube, s,s,s,p,p,d,d,f spherical, 4 primitives, "
+                               "nao 5200, 2 densities, tau 1e-11, every %d-th canonical bra pair (%d of %d)"
+                               % (args.sph_stride, len(bras), nbra),
+                   "quartets_per_step": q32 // st, "l2": "flushed between steps (512 MB write)"},
+        "fp64": {"value": q64 / (ms64 * 1e-3), "unit": "quartets/s", "ms_per_step": ms64 / st,
+                 "mixed_speedup": ms64 / ms32},
+        "energy_error_mixed_vs_fp64_Eh_on_sample": dE,
+        "estimated_full_build_s": {"mixed": args.sph_stride * ms32 / st * 1e-3,
+                                   "fp64": args.sph_stride * ms64 / st * 1e-3,
+                                   "basis": "stride x sampled time (interleaved share of the bra pairs)"},
+        "clocks": clocks,
+        "gpu_launches": l32,
     }
     print(json.dumps(line))
 
@@ -398,6 +480,8 @@ def main():
         return grad_bench(args)
     if args.workload == "dense":
         return dense_bench(args)
+    if args.workload == "jk-sph":
+        return jk_sph_bench(args)
     if args.impl == "reference":
         return reference_arm(args)
     import torch
