@@ -1413,8 +1413,9 @@ int igpu_grad_device(igpu_plan* P, const igpu_term* coulomb, int ncoul, const ig
   if (precision != IGPU_PRECISION_FP64 && precision != IGPU_PRECISION_MIXED)
     return fail(IGPU_ERR_INVALID_ARGUMENT, "unknown precision");
   if (std::isnan(threshold)) return fail(IGPU_ERR_INVALID_ARGUMENT, "threshold is NaN");
-  // DirectGradContractor::new (src/direct_grad.rs:181-186)
-  for (const DevShell& d : P->shells) {
+  // DirectGradContractor::new (src/direct_grad.rs:181-186), main shells only
+  for (int sh = 0; sh < P->nsh; ++sh) {
+    const DevShell& d = P->shells[sh];
     if (d.l > MAX_GRAD_L)
       return fail(IGPU_ERR_ANGULAR_MOMENTUM_GRAD, "angular momentum too high for the gradient (l <= 5)");
     if (d.l > GRAD_KERNEL_MAX_L)

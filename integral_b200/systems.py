@@ -223,3 +223,17 @@ def df_system(seed: int = 6, natom: int = 5, side: float = 7.0, spherical: bool 
             aux.append(dict(l=L_OF[letter], spherical=spherical, center=[float(x) for x in c],
                             exps=[float(e)], coefs=[1.0]))
     return dict(name="df_%datom" % natom, main=main, aux=aux, seed=seed)
+
+
+def grad_extended_fixture():
+    """tests/direct_grad_contractor.rs:636-660: four atoms 8.5 to 19.3 bohr
+    apart with diffuse valence shells (s of 2 primitives, p, and a spherical
+    d on every other atom), so shell-pair overlaps span many orders."""
+    atoms = [[0.0, 0.0, 0.0], [8.5, 0.0, 0.5], [8.0, 9.0, -0.4], [19.0, 3.0, 1.0]]
+    shells = []
+    for a, at in enumerate(atoms):
+        shells.append(dict(l=0, spherical=False, center=at, exps=[1.2, 0.25], coefs=[0.5, 0.6]))
+        shells.append(dict(l=1, spherical=False, center=at, exps=[0.3], coefs=[1.0]))
+        if a % 2 == 0:
+            shells.append(dict(l=2, spherical=True, center=at, exps=[0.28], coefs=[1.0]))
+    return shells

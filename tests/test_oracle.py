@@ -466,3 +466,45 @@ def test_direct_gradient_matches_dense_gamma_contraction(spherical, engine, omeg
     assert float(np.max(np.abs(g - ref))) < 1e-10
     assert float(np.max(np.abs(g.sum(axis=0)))) < 1e-10
     assert float(np.max(np.abs(g))) > 1e-3
+
+
+def test_gradient_term_lists_are_additive_and_bra_order_free():
+    # tests/direct_grad_contractor.rs:556-612: coulomb-only + exchange-only
+    # = both; no terms = exact zero; bra tasks summed in reverse order over
+    # two partial outputs = the serial contraction
+    shells = S.direct_grad_fixture(True)
+    B = O.OracleBasis(shells)
+    coul, exch = S.grad_fixture_terms(B.nao)
+    both, _, _ = B.direct_grad(coul, exch, 0.0)
+    c_only, _, _ = B.direct_grad(coul, [], 0.0)
+    x_only, _, _ = B.direct_grad([], exch, 0.0)
+    assert float(np.max(np.abs(c_only))) > 1e-3 and float(np.max(np.abs(x_only))) > 1e-3
+    assert float(np.max(np.abs(c_only + x_only - both))) < 1e-12
+    nothing, _, _ = B.direct_grad([], [], 0.0)
+    assert np.all(nothing == 0.0)
+    p = S.grad_symmetric(B.nao, 4)
+    terms = [(1.0, p, p)]
+    serial, _, _ = B.direct_grad(terms, terms, 0.0)
+    nbra = len(shells) * (len(shells) + 1) // 2
+    rev = np.arange(nbra)[::-1]
+    parts = [B.direct_grad(terms, terms, 0.0, bras=rev[t::2])[0] for t in range(2)]
+    assert float(np.max(np.abs(parts[0] + parts[1] - serial))) < 1e-12
+
+
+def test_gradient_screening_error_is_bounded_on_extended_system():
+    # tests/direct_grad_contractor.rs:662-690: tau = 0 equals the dense
+    # contraction; the screened error stays below 100 tau; tau = inf drops
+    # every quartet
+    shells = S.grad_extended_fixture()
+    B = O.OracleBasis(shells)
+    n = B.nao
+    coul, exch = S.grad_fixture_terms(n)
+    ref = B.eri_grad_contract(_dense_gamma(n, coul, exch))
+    exact, _, _ = B.direct_grad(coul, exch, 0.0)
+    assert float(np.max(np.abs(exact))) > 1e-3
+    assert float(np.max(np.abs(exact - ref))) < 1e-10
+    for thr in (1e-12, 1e-9, 1e-6):
+        screened, _, _ = B.direct_grad(coul, exch, thr)
+        assert float(np.max(np.abs(screened - exact))) < 100.0 * thr
+    nothing, cnt, _ = B.direct_grad(coul, exch, float("inf"))
+    assert cnt == 0 and np.all(nothing == 0.0)
