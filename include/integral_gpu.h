@@ -147,6 +147,15 @@ int igpu_eri_dense(igpu_plan* plan, double* out);
  * ket pairs scattered into the 4 bra/ket-internal slots of the host nao^4
  * buffer (assigned; other elements untouched). */
 int igpu_eri_builder_fill(igpu_plan* plan, const uint32_t* bra_subset, size_t nsub, double* out);
+/* Basis::eri_screened (src/integrals.rs:864-981): the dense tensor with
+ * every canonical quartet of Q_ij*Q_kl < tau left zero in all its
+ * permutation slots; *total and *skipped (either may be NULL) receive the
+ * ScreeningStats counts of canonical quartets.  NaN tau is rejected. */
+int igpu_eri_screened(igpu_plan* plan, double tau, double* out, uint64_t* total, uint64_t* skipped);
+/* Basis::eri_block (src/integrals.rs:600-640): the (ij|kl) block of shells
+ * i, j, k, l in that order, row-major [n_i][n_j][n_k][n_l] over the shells'
+ * functions; out holds n_i*n_j*n_k*n_l doubles (host). */
+int igpu_eri_block(igpu_plan* plan, int i, int j, int k, int l, double* out);
 /* PackedEriBuilder::build / fill (src/packed_eri.rs:156-237): the
  * symmetry-unique tensor, AO pairs numbered shell-pair blocked (canonical
  * shell pair, then (a, b) row-major with b <= a on diagonal pairs, see

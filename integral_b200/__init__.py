@@ -89,6 +89,20 @@ def _omega_of(kernel) -> float:
     return 0.0 if kernel is None else float(kernel.omega)
 
 
+@dataclass
+class ScreeningStats:
+    """Outcome of a Schwarz-screened dense build (src/integrals.rs:983-1005):
+    canonical shell quartets considered and skipped, and tau."""
+    shell_quartets_total: int
+    shell_quartets_skipped: int
+    tau: float
+
+    def skipped_fraction(self) -> float:
+        if self.shell_quartets_total == 0:
+            return 0.0
+        return self.shell_quartets_skipped / self.shell_quartets_total
+
+
 def n_cart(l: int) -> int:
     return (l + 1) * (l + 2) // 2
 
@@ -276,6 +290,34 @@ class Basis:
         finally:
             p.set_erf_omega(0.0)
         return out
+
+    def eri_block(self, i: int, j: int, k: int, l: int) -> np.ndarray:
+        """Basis::eri_block (src/integrals.rs:600-619): the (ij|kl) block,
+        row-major [n_i][n_j][n_k][n_l] over the shells' functions."""
+        return self.eri_block_with(Engine.Auto, i, j, k, l)
+
+    def eri_block_with(self, engine: Engine, i: int, j: int, k: int, l: int) -> np.ndarray:
+        nsh = len(self._shells)
+        if not all(0 <= x < nsh for x in (i, j, k, l)):
+            raise IntegralError(-1, "invalid argument", "shell index out of range")
+        p = self.plan(engine)
+        out = np.empty(int(np.prod([self._shells[x].n_func() for x in (i, j, k, l)])))
+        _lib.check(_lib.lib().igpu_eri_block(p.h, i, j, k, l, out.ctypes.data_as(c_double_p)))
+        return out
+
+    def eri_screened(self, tau: float):
+        """Basis::eri_screened (src/integrals.rs:864-981): the dense tensor
+        with canonical quartets of Q_ij*Q_kl < tau left zero, and its
+        ScreeningStats."""
+        return self.eri_screened_with(Engine.Auto, tau)
+
+    def eri_screened_with(self, engine: Engine, tau: float):
+        p = self.plan(engine)
+        out = np.empty(p.nao ** 4)
+        total, skipped = ctypes.c_uint64(), ctypes.c_uint64()
+        _lib.check(_lib.lib().igpu_eri_screened(p.h, float(tau), out.ctypes.data_as(c_double_p),
+                                                ctypes.byref(total), ctypes.byref(skipped)))
+        return out, ScreeningStats(total.value, skipped.value, float(tau))
 
     def eri_with(self, engine: Engine) -> np.ndarray:
         p = self.plan(engine)

@@ -71,6 +71,9 @@ def lib():
     L.igpu_eri_dense.argtypes = [vp, c_double_p]
     L.igpu_eri_builder_fill.argtypes = [vp, c_u32_p, ctypes.c_size_t, c_double_p]
     L.igpu_eri_packed.argtypes = [vp, ctypes.c_double, c_u32_p, ctypes.c_size_t, c_double_p]
+    L.igpu_eri_screened.argtypes = [vp, ctypes.c_double, c_double_p, ctypes.POINTER(ctypes.c_uint64),
+                                    ctypes.POINTER(ctypes.c_uint64)]
+    L.igpu_eri_block.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_double_p]
     L.igpu_plan_attach_aux.argtypes = [vp, ctypes.POINTER(IgpuShell), ctypes.c_size_t]
     L.igpu_aux_query.argtypes = [vp, c_size_p, c_size_p]
     L.igpu_schwarz_aux.argtypes = [vp, c_double_p]
@@ -96,7 +99,7 @@ EXPORTED = [
     "igpu_abi_version", "igpu_last_error_string", "igpu_plan_create", "igpu_plan_destroy", "igpu_plan_query",
     "igpu_bra_pairs", "igpu_atoms", "igpu_schwarz", "igpu_set_mixed_cutoff", "igpu_set_erf_omega",
     "igpu_eri_dense",
-    "igpu_eri_builder_fill", "igpu_eri_packed", "igpu_plan_attach_aux", "igpu_aux_query", "igpu_schwarz_aux",
+    "igpu_eri_builder_fill", "igpu_eri_screened", "igpu_eri_block", "igpu_eri_packed", "igpu_plan_attach_aux", "igpu_aux_query", "igpu_schwarz_aux",
     "igpu_eri_2c", "igpu_eri_3c", "igpu_density_shell_bounds", "igpu_jk", "igpu_jk_device", "igpu_jk_device_static",
     "igpu_grad",
     "igpu_grad_device", "igpu_last_stats", "igpu_last_profile",

@@ -99,6 +99,7 @@ enum Mode : int {
   MODE_PACKED = 5,
   MODE_DF3 = 6,  // density fitting (mu nu|P): main pair x (aux shell, unit s)
   MODE_DF2 = 7,  // density fitting (P|Q): (aux shell, unit s) x (aux shell, unit s)
+  MODE_BLOCK = 8,  // one shell-quartet block in a requested shell order
 };
 
 struct JKDev {
@@ -170,8 +171,10 @@ struct KernelArgs {
   int kinds;             // 0 all shells Cartesian, 1 all spherical, 2 mixed
   double omega;          // 0: Coulomb 1/r; > 0: long-range erf(omega r)/r
   int naux;              // MODE_DF3 / MODE_DF2: auxiliary functions
-  size_t dense_len;      // MODE_DF3 / MODE_DF2: doubles in `dense`
-  unsigned* store_fault; // MODE_DF3 / MODE_DF2: set when an index falls outside `dense`
+  size_t dense_len;      // MODE_DF3 / MODE_DF2 / MODE_BLOCK: doubles in `dense`
+  unsigned* store_fault; // MODE_DF3 / MODE_DF2 / MODE_BLOCK: set when an index falls outside `dense`
+  int blk_shells[4];     // MODE_BLOCK: requested shells (i, j, k, l)
+  int blk_dims[4];       // MODE_BLOCK: their function counts
 };
 
 }  // namespace igpu

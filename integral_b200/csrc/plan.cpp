@@ -955,9 +955,54 @@ int igpu_jk_device_static(igpu_plan* P, const double* d_dens, int ndens, double 
   return IGPU_OK;
 }
 
-// Dense tensor (MODE_DENSE, every canonical quartet, no screening) or the
-// EriBuilder fill (MODE_BUILDER, every ket for the requested bras).
-static int dense_like(igpu_plan* P, bool builder, const uint32_t* sub, size_t nsub, double* out) {
+namespace {
+
+// One launch whose ket list is owned by the launch: bra b runs kets
+// kets[0 .. nket[b]-1].
+std::unique_ptr<Launch> owned_launch(igpu_plan* P, int pcb, int pck, const std::vector<int>& bras,
+                                     const std::vector<int>& nket, const std::vector<int>& kets, int& rc) {
+  auto L = make_launch(P, pcb, pck, false, bras, nket, {}, nullptr, 0, P->stream, rc);
+  if (!L) return nullptr;
+  cudaError_t e = L->own_kets.upload(kets, P->stream);
+  if (e != cudaSuccess) {
+    rc = cuda_fail(e, "ket list upload");
+    return nullptr;
+  }
+  L->ket_list = L->own_kets.p;
+  return L;
+}
+
+// Runs a density-fitting task set into d_dense (len doubles) and checks the
+// writers' fault flag.
+int run_df(igpu_plan* P, TaskSet& ts, int mode, size_t len) {
+  CK(P->d_fault.ensure(1));
+  CK(cudaMemsetAsync(P->d_fault.p, 0, sizeof(unsigned), P->stream));
+  KernelArgs A = base_args(P);
+  A.mode = mode;
+  A.dense = P->d_dense.p;
+  A.dense_len = len;
+  A.naux = P->naux;
+  A.store_fault = P->d_fault.p;
+  A.counters = nullptr;
+  uint32_t launches = 0;
+  int rc = run_tasks(P, ts, A, P->stream, launches);
+  if (rc) return rc;
+  unsigned fault = 0;
+  CK(cudaMemcpyAsync(&fault, P->d_fault.p, sizeof(unsigned), cudaMemcpyDeviceToHost, P->stream));
+  CK(cudaStreamSynchronize(P->stream));
+  if (fault) return fail(IGPU_ERR_CUDA, "internal: density-fitting store outside the output");
+  P->last = igpu_stats{};
+  P->last.launches = launches;
+  return IGPU_OK;
+}
+
+}  // namespace
+
+// Dense tensor (MODE_DENSE: every canonical quartet, or with tau > -inf the
+// quartets with Q_ij*Q_kl >= tau) or the EriBuilder fill (MODE_BUILDER,
+// every ket for the requested bras).
+static int dense_like(igpu_plan* P, bool builder, const uint32_t* sub, size_t nsub, double* out,
+                      double tau = -std::numeric_limits<double>::infinity()) {
   if (!P || !out) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
   const size_t n = (size_t)P->nao;
   const size_t n4 = n * n * n * n;
@@ -970,7 +1015,18 @@ static int dense_like(igpu_plan* P, bool builder, const uint32_t* sub, size_t ns
   TaskSet* ts = &local;
   const int npc = (int)P->class_pairs.size();
   int rc = IGPU_OK;
-  if (!builder) {
+  if (!builder && tau > -std::numeric_limits<double>::infinity()) {
+    auto key = std::make_pair(tau, 0.0);
+    auto it = P->jk_tasks.find(key);
+    if (it == P->jk_tasks.end()) {
+      auto t = std::make_unique<TaskSet>();
+      rc = build_jk_tasks(P, tau, 0.0, *t);
+      if (rc) return rc;
+      CK(cudaStreamSynchronize(P->stream));
+      it = P->jk_tasks.emplace(key, std::move(t)).first;
+    }
+    ts = it->second.get();
+  } else if (!builder) {
     if (!P->dense_tasks) {
       P->dense_tasks = std::make_unique<TaskSet>();
       rc = build_jk_tasks(P, -std::numeric_limits<double>::infinity(), 0.0, *P->dense_tasks);
@@ -1041,6 +1097,62 @@ int igpu_eri_builder_fill(igpu_plan* P, const uint32_t* sub, size_t nsub, double
   return dense_like(P, true, sub, nsub, out);
 }
 
+int igpu_eri_screened(igpu_plan* P, double tau, double* out, uint64_t* total, uint64_t* skipped) {
+  if (!P || !out) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (std::isnan(tau)) return fail(IGPU_ERR_INVALID_ARGUMENT, "tau is NaN");
+  int rc = dense_like(P, false, nullptr, 0, out, tau);
+  if (rc) return rc;
+  // canonical quartets i >= j, k >= l, ij >= kl (integrals.rs:897-910)
+  const uint64_t all = (uint64_t)P->npairs * ((uint64_t)P->npairs + 1) / 2;
+  if (total) *total = all;
+  if (skipped) *skipped = all - P->last.quartets;
+  return IGPU_OK;
+}
+
+int igpu_eri_block(igpu_plan* P, int i, int j, int k, int l, double* out) {
+  if (!P || !out) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  const int sh4[4] = {i, j, k, l};
+  for (int x : sh4)
+    if (x < 0 || x >= P->nsh) return fail(IGPU_ERR_INVALID_ARGUMENT, "shell index out of range");
+  const int pb = std::max(i, j) * (std::max(i, j) + 1) / 2 + std::min(i, j);
+  const int pk = std::max(k, l) * (std::max(k, l) + 1) / 2 + std::min(k, l);
+  size_t len = 1;
+  KernelArgs A = base_args(P);
+  for (int x = 0; x < 4; ++x) {
+    A.blk_shells[x] = sh4[x];
+    A.blk_dims[x] = P->shells[sh4[x]].nfunc;
+    len *= (size_t)A.blk_dims[x];
+  }
+  CK(P->d_dense.ensure(len));
+  CK(cudaMemsetAsync(P->d_dense.p, 0, len * sizeof(double), P->stream));
+  CK(P->d_fault.ensure(1));
+  CK(cudaMemsetAsync(P->d_fault.p, 0, sizeof(unsigned), P->stream));
+  // the larger pair class is the evaluation bra
+  const int cb = P->pairs[pb].cls, ck = P->pairs[pk].cls;
+  const bool swap = ck > cb;
+  TaskSet ts;
+  int rc;
+  auto L = owned_launch(P, swap ? ck : cb, swap ? cb : ck, {swap ? pk : pb}, {1}, {swap ? pb : pk}, rc);
+  if (!L) return rc;
+  ts.launches.push_back(std::move(L));
+  A.mode = MODE_BLOCK;
+  A.dense = P->d_dense.p;
+  A.dense_len = len;
+  A.store_fault = P->d_fault.p;
+  A.counters = nullptr;
+  uint32_t launches = 0;
+  rc = run_tasks(P, ts, A, P->stream, launches);
+  if (rc) return rc;
+  unsigned fault = 0;
+  CK(cudaMemcpyAsync(&fault, P->d_fault.p, sizeof(unsigned), cudaMemcpyDeviceToHost, P->stream));
+  CK(cudaMemcpyAsync(out, P->d_dense.p, len * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
+  CK(cudaStreamSynchronize(P->stream));
+  if (fault) return fail(IGPU_ERR_CUDA, "internal: block store outside the output");
+  P->last = igpu_stats{};
+  P->last.launches = launches;
+  return IGPU_OK;
+}
+
 int igpu_eri_packed(igpu_plan* P, double threshold, const uint32_t* sub, size_t nsub, double* out) {
   if (!P || !out) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
   if (std::isnan(threshold)) return fail(IGPU_ERR_INVALID_ARGUMENT, "threshold is NaN");
@@ -1109,49 +1221,6 @@ int igpu_eri_packed(igpu_plan* P, double threshold, const uint32_t* sub, size_t 
 }
 
 // ===================================================== density fitting (df.rs)
-
-namespace {
-
-// One launch whose ket list is owned by the launch: bra b runs kets
-// kets[0 .. nket[b]-1].
-std::unique_ptr<Launch> owned_launch(igpu_plan* P, int pcb, int pck, const std::vector<int>& bras,
-                                     const std::vector<int>& nket, const std::vector<int>& kets, int& rc) {
-  auto L = make_launch(P, pcb, pck, false, bras, nket, {}, nullptr, 0, P->stream, rc);
-  if (!L) return nullptr;
-  cudaError_t e = L->own_kets.upload(kets, P->stream);
-  if (e != cudaSuccess) {
-    rc = cuda_fail(e, "ket list upload");
-    return nullptr;
-  }
-  L->ket_list = L->own_kets.p;
-  return L;
-}
-
-// Runs a density-fitting task set into d_dense (len doubles) and checks the
-// writers' fault flag.
-int run_df(igpu_plan* P, TaskSet& ts, int mode, size_t len) {
-  CK(P->d_fault.ensure(1));
-  CK(cudaMemsetAsync(P->d_fault.p, 0, sizeof(unsigned), P->stream));
-  KernelArgs A = base_args(P);
-  A.mode = mode;
-  A.dense = P->d_dense.p;
-  A.dense_len = len;
-  A.naux = P->naux;
-  A.store_fault = P->d_fault.p;
-  A.counters = nullptr;
-  uint32_t launches = 0;
-  int rc = run_tasks(P, ts, A, P->stream, launches);
-  if (rc) return rc;
-  unsigned fault = 0;
-  CK(cudaMemcpyAsync(&fault, P->d_fault.p, sizeof(unsigned), cudaMemcpyDeviceToHost, P->stream));
-  CK(cudaStreamSynchronize(P->stream));
-  if (fault) return fail(IGPU_ERR_CUDA, "internal: density-fitting store outside the output");
-  P->last = igpu_stats{};
-  P->last.launches = launches;
-  return IGPU_OK;
-}
-
-}  // namespace
 
 int igpu_plan_attach_aux(igpu_plan* P, const igpu_shell* aux, size_t naux_sh) {
   if (!P) return fail(IGPU_ERR_INVALID_ARGUMENT, "plan is NULL");

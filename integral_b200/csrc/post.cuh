@@ -637,8 +637,8 @@ __device__ __forceinline__ void consume_packed(const KernelArgs& A, const double
   }
 }
 
-// Store of the density-fitting writers: an index outside the output raises
-// the launch's fault flag instead of writing.
+// Store of the density-fitting and block writers: an index outside the
+// output raises the launch's fault flag instead of writing.
 __device__ __forceinline__ void df_store(const KernelArgs& A, size_t at, double v) {
   if (at < A.dense_len)
     A.dense[at] = v;
@@ -700,6 +700,35 @@ __device__ __forceinline__ void consume_df2(const KernelArgs& A, const double* B
   }
 }
 
+// One shell-quartet block (Basis::eri_block, src/integrals.rs:600-640): the
+// evaluated quartet is one of the 8 permutations of the requested
+// (i, j, k, l).  The first permutation whose shells match maps every
+// evaluated element to the requested row-major [n_i][n_j][n_k][n_l] block.
+__device__ __forceinline__ void consume_block(const KernelArgs& A, const double* B, const int dims[4],
+                                              const int sh[4], int lane, int T) {
+  // P8[p][r]: evaluation slot of requested position r under permutation p
+  const int P8[8][4] = {{0, 1, 2, 3}, {1, 0, 2, 3}, {0, 1, 3, 2}, {1, 0, 3, 2},
+                        {2, 3, 0, 1}, {3, 2, 0, 1}, {2, 3, 1, 0}, {3, 2, 1, 0}};
+  int pick = -1;
+  for (int p = 0; p < 8 && pick < 0; ++p)
+    if (sh[P8[p][0]] == A.blk_shells[0] && sh[P8[p][1]] == A.blk_shells[1] && sh[P8[p][2]] == A.blk_shells[2] &&
+        sh[P8[p][3]] == A.blk_shells[3])
+      pick = p;
+  if (pick < 0) {
+    if (lane == 0) atomicOr(A.store_fault, 2u);
+    return;
+  }
+  const int* m = P8[pick];
+  const int total = dims[0] * dims[1] * dims[2] * dims[3];
+  for (int q = lane; q < total; q += T) {
+    int idx[4];
+    block_index(q, dims, idx);
+    const size_t at =
+        (((size_t)idx[m[0]] * A.blk_dims[1] + idx[m[1]]) * A.blk_dims[2] + idx[m[2]]) * A.blk_dims[3] + idx[m[3]];
+    df_store(A, at, B[q]);
+  }
+}
+
 // Schwarz: sqrt(max |(mu nu|mu nu)|) over the function-space diagonal of the
 // (ij|ij) block (src/integrals.rs:850-860).
 __device__ __forceinline__ void consume_schwarz(const KernelArgs& A, const double* B, const int dims[4],
@@ -758,6 +787,9 @@ __device__ __forceinline__ void post_quartet(const KernelArgs& A, const ClassDim
       break;
     case MODE_DF2:
       consume_df2(A, B, dims, offs, shl, lane, T);
+      break;
+    case MODE_BLOCK:
+      consume_block(A, B, dims, shl, lane, T);
       break;
     default:
       break;

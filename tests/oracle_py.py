@@ -132,6 +132,28 @@ class OracleBasis:
         lib().orc_eri(self.h, ENGINES[engine], _dp(out))
         return out
 
+    def eri_screened(self, tau, engine="auto"):
+        """Basis::eri_screened_with (src/integrals.rs:880-981): the dense
+        tensor with every canonical quartet of Q_ij*Q_kl < tau left zero in
+        all its permutation slots; returns (tensor, total, skipped) over the
+        canonical quartets.  The bound is permutation-invariant, so the mask
+        is taken over all ordered shell quartets."""
+        E = self.eri(engine)
+        Q = self.schwarz(engine)
+        n = self.nsh
+        keep = np.multiply.outer(Q, Q) >= tau  # [i, j, k, l]
+        nf = [(2 * s["l"] + 1) if s.get("spherical") else (s["l"] + 1) * (s["l"] + 2) // 2 for s in self.shells]
+        owner = np.repeat(np.arange(n), nf)
+        K = keep[np.ix_(owner, owner, owner, owner)]
+        pairs = [(i, j) for i in range(n) for j in range(i + 1)]
+        total = skipped = 0
+        for p, (i, j) in enumerate(pairs):
+            for (k, l) in pairs[:p + 1]:
+                total += 1
+                if Q[i, j] * Q[k, l] < tau:
+                    skipped += 1
+        return np.where(K.reshape(-1), E, 0.0), total, skipped
+
     def eri_block(self, i, j, k, l, engine="auto"):
         nf = [(2 * s["l"] + 1) if s.get("spherical") else (s["l"] + 1) * (s["l"] + 2) // 2
               for s in (self.shells[i], self.shells[j], self.shells[k], self.shells[l])]

@@ -508,3 +508,31 @@ def test_gradient_screening_error_is_bounded_on_extended_system():
         assert float(np.max(np.abs(screened - exact))) < 100.0 * thr
     nothing, cnt, _ = B.direct_grad(coul, exch, float("inf"))
     assert cnt == 0 and np.all(nothing == 0.0)
+
+
+
+# ------------------------------------------------- screened dense tensor
+
+def test_screened_tensor_keeps_retained_elements_and_bounds_the_rest():
+    # tests/screening.rs: |(mu nu|la si)| <= Q_ij Q_kl element-wise, the
+    # screened tensor equals the unscreened one on retained elements, and
+    # tau = 0 is the unscreened tensor
+    s = S.dense_eri_system()
+    B = O.OracleBasis(s["shells"])
+    E = B.eri()
+    Q = B.schwarz()
+    n = B.nsh
+    nf = [3 if sh["l"] == 1 else 1 for sh in s["shells"]]
+    owner = np.repeat(np.arange(n), nf)
+    bound = np.multiply.outer(Q, Q)[np.ix_(owner, owner, owner, owner)].reshape(-1)
+    assert np.all(np.abs(E) <= bound * (1 + 1e-12) + 1e-15)
+    E0, total, skipped = B.eri_screened(0.0)
+    assert np.array_equal(E0, E) and skipped == 0
+    npairs = n * (n + 1) // 2
+    assert total == npairs * (npairs + 1) // 2 == 108345
+    tau = 1e-4
+    Es, total, skipped = B.eri_screened(tau)
+    assert 0 < skipped < total
+    kept = Es != 0.0
+    assert np.array_equal(Es[kept], E[kept])
+    assert float(np.max(np.abs(E[~kept]))) < tau
