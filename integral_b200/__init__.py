@@ -136,6 +136,11 @@ class Shell:
         return cls(l, center, exponents, coefficients, ShellKind.Spherical)
 
     @classmethod
+    def with_kind(cls, l, center, exponents, coefficients, kind: ShellKind):
+        """Shell::with_kind (src/shell.rs:92-118)."""
+        return cls(l, center, exponents, coefficients, kind)
+
+    @classmethod
     def from_dict(cls, d):
         return cls(d["l"], d["center"], d["exps"], d["coefs"],
                    ShellKind.Spherical if d.get("spherical") else ShellKind.Cartesian)
@@ -327,10 +332,19 @@ class Basis:
         return out
 
     def schwarz_bounds(self) -> np.ndarray:
-        p = self.plan(Engine.Auto)
+        """Basis::schwarz_bounds (src/integrals.rs:835-862): nsh x nsh,
+        row-major, evaluated on the device at plan creation."""
+        return self.schwarz_bounds_with(Engine.Auto)
+
+    def schwarz_bounds_with(self, engine: Engine) -> np.ndarray:
+        p = self.plan(engine)
         q = np.empty(p.nsh * p.nsh)
         _lib.check(_lib.lib().igpu_schwarz(p.h, q.ctypes.data_as(c_double_p)))
         return q
+
+    def eri_builder(self) -> "EriBuilder":
+        """Basis::eri_builder (src/eri_builder.rs:575-577): EriBuilder::new(self)."""
+        return EriBuilder(self)
 
     def direct_contractor(self) -> "DirectContractor":
         return DirectContractor(self)
@@ -429,6 +443,10 @@ class EriBuilder:
         self._plan = basis.plan(engine)
         self._pairs = self._plan.bra_pairs()
         self._omega = 0.0
+
+    @classmethod
+    def new(cls, basis):
+        return cls(basis)
 
     @classmethod
     def with_engine(cls, basis, engine):

@@ -81,6 +81,8 @@ def test_python_shell_validation_mirrors_reference():
     assert e.value.code == -4
     s = ib.Shell.new_spherical(3, [0, 0, 0], [1.0], [1.0])
     assert s.n_func() == 7 and s.n_cart() == 10
+    s = ib.Shell.with_kind(2, [0, 0, 0], [1.0], [1.0], ib.ShellKind.Spherical)
+    assert s.n_func() == 5 and s.kind() == ib.ShellKind.Spherical
 
 
 def test_erf_kernel_requires_finite_positive_omega():
