@@ -85,6 +85,25 @@ class EriKernel:
 EriKernel.Coulomb = EriKernel(0.0)
 
 
+def select_engine(ne: int, nf: int, contraction_degree: int) -> Engine:
+    """select_engine (src/integrals.rs:374-388): the reference's CPU engine
+    policy for a quartet of bra / ket angular sums ne, nf and primitive
+    product contraction_degree: OS/HGP from degree 1 up to l_total 5, from
+    degree 3 up to l_total 16 when max(ne, nf) <= 6, from degree 16 above
+    that, Rys for l_total >= 17.  Kept for API parity: the GPU evaluates
+    every class with its Rys kernels whatever this returns."""
+    l_total = ne + nf
+    if l_total >= 17:
+        return Engine.Rys
+    if l_total <= 5:
+        threshold = 1
+    elif max(ne, nf) <= 6:
+        threshold = 3
+    else:
+        threshold = 16
+    return Engine.OsHgp if contraction_degree >= threshold else Engine.Rys
+
+
 def _omega_of(kernel) -> float:
     return 0.0 if kernel is None else float(kernel.omega)
 

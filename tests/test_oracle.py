@@ -536,3 +536,14 @@ def test_screened_tensor_keeps_retained_elements_and_bounds_the_rest():
     kept = Es != 0.0
     assert np.array_equal(Es[kept], E[kept])
     assert float(np.max(np.abs(E[~kept]))) < tau
+
+
+
+def test_select_engine_policy_matches_the_oracle():
+    # src/integrals.rs:374-388 (tests/dispatch.rs: every threshold boundary)
+    import integral_b200 as ib
+    for ne in range(0, 13):
+        for nf in range(0, 13):
+            for deg in (1, 2, 3, 4, 15, 16, 17, 81, 256):
+                want = {"os": ib.Engine.OsHgp, "rys": ib.Engine.Rys}[O.select_engine(ne, nf, deg)]
+                assert ib.select_engine(ne, nf, deg) == want, (ne, nf, deg)
