@@ -129,6 +129,9 @@ struct igpu_plan {
   DevBuf<unsigned long long> d_flag;
   DevBuf<unsigned> d_bitmap;
   std::map<std::pair<double, double>, std::unique_ptr<TaskSet>> jk_tasks;  // (threshold, fp64 cutoff)
+  // mixed-precision keys in insertion order: their cutoff follows max|D|,
+  // so every new density would add one; at most kMixedTaskSets are kept
+  std::vector<std::pair<double, double>> mixed_keys;
   std::unique_ptr<TaskSet> dense_tasks;
   double mixed_cutoff = 1e-4;
   double erf_omega = 0.0;  // 0: Coulomb; > 0: erf(omega r)/r for every later call
@@ -155,6 +158,9 @@ struct igpu_plan {
 };
 
 namespace {
+
+// Mixed-precision J/K task lists kept per plan (see igpu_plan::mixed_keys).
+constexpr size_t kMixedTaskSets = 4;
 
 // Upload the angular tables and the Rys tables to this device once.
 int ensure_constants(int dev) {
@@ -482,6 +488,35 @@ int build_jk_tasks(igpu_plan* P, double tau, double fp64_cut, TaskSet& ts) {
       }
     }
   return IGPU_OK;
+}
+
+// The task list of (threshold, fp64 cutoff), built on first use and cached.
+// A mixed list's cutoff follows the maximum of the density (or term
+// matrices), so only the kMixedTaskSets most recent mixed lists are kept;
+// FP64 lists (cutoff 0, one per threshold) stay.  Every entry point
+// synchronises before it returns, so an evicted list has no launch in
+// flight.
+TaskSet* cached_tasks(igpu_plan* P, double threshold, double fp64_cut, int& rc) {
+  rc = IGPU_OK;
+  const auto key = std::make_pair(threshold, fp64_cut);
+  auto it = P->jk_tasks.find(key);
+  if (it != P->jk_tasks.end()) return it->second.get();
+  if (fp64_cut > 0.0 && P->mixed_keys.size() >= kMixedTaskSets) {
+    P->jk_tasks.erase(P->mixed_keys.front());
+    P->mixed_keys.erase(P->mixed_keys.begin());
+  }
+  auto ts = std::make_unique<TaskSet>();
+  rc = build_jk_tasks(P, threshold, fp64_cut, *ts);
+  if (rc) return nullptr;
+  cudaError_t e = cudaStreamSynchronize(P->stream);
+  if (e != cudaSuccess) {
+    rc = cuda_fail(e, "task list upload");
+    return nullptr;
+  }
+  TaskSet* out = ts.get();
+  P->jk_tasks.emplace(key, std::move(ts));
+  if (fp64_cut > 0.0) P->mixed_keys.push_back(key);
+  return out;
 }
 
 int check_bra_subset(igpu_plan* P, const uint32_t* sub, size_t nsub, std::vector<unsigned>& bitmap) {
@@ -817,15 +852,9 @@ int igpu_jk_device(igpu_plan* P, const double* d_dens, int ndens, const uint32_t
   } else {
     CK(cudaStreamSynchronize(s));
   }
-  auto key = std::make_pair(threshold, fp64_cut);
-  auto it = P->jk_tasks.find(key);
-  if (it == P->jk_tasks.end()) {
-    auto ts = std::make_unique<TaskSet>();
-    int rc = build_jk_tasks(P, threshold, fp64_cut, *ts);
-    if (rc) return rc;
-    CK(cudaStreamSynchronize(P->stream));
-    it = P->jk_tasks.emplace(key, std::move(ts)).first;
-  }
+  int trc;
+  TaskSet* tasks = cached_tasks(P, threshold, fp64_cut, trc);
+  if (!tasks) return trc;
   KernelArgs A = base_args(P);
   A.mode = MODE_JK;
   A.jk.D = d_dens;
@@ -851,7 +880,7 @@ int igpu_jk_device(igpu_plan* P, const double* d_dens, int ndens, const uint32_t
     A.jk.K = want_k ? d_K : nullptr;
   }
   uint32_t launches = 3;
-  int rc = run_tasks(P, *it->second, A, s, launches);
+  int rc = run_tasks(P, *tasks, A, s, launches);
   if (rc) return rc;
   if (A.jk.symmetric) {
     CK(launch_symmetrize_add(P->d_Jh.p, d_J, ndens, P->nao, s));
@@ -1016,16 +1045,8 @@ static int dense_like(igpu_plan* P, bool builder, const uint32_t* sub, size_t ns
   const int npc = (int)P->class_pairs.size();
   int rc = IGPU_OK;
   if (!builder && tau > -std::numeric_limits<double>::infinity()) {
-    auto key = std::make_pair(tau, 0.0);
-    auto it = P->jk_tasks.find(key);
-    if (it == P->jk_tasks.end()) {
-      auto t = std::make_unique<TaskSet>();
-      rc = build_jk_tasks(P, tau, 0.0, *t);
-      if (rc) return rc;
-      CK(cudaStreamSynchronize(P->stream));
-      it = P->jk_tasks.emplace(key, std::move(t)).first;
-    }
-    ts = it->second.get();
+    ts = cached_tasks(P, tau, 0.0, rc);
+    if (!ts) return rc;
   } else if (!builder) {
     if (!P->dense_tasks) {
       P->dense_tasks = std::make_unique<TaskSet>();
@@ -1186,16 +1207,8 @@ int igpu_eri_packed(igpu_plan* P, double threshold, const uint32_t* sub, size_t 
   TaskSet* ts = nullptr;
   int rc = IGPU_OK;
   if (threshold > 0.0) {
-    auto key = std::make_pair(threshold, 0.0);
-    auto it = P->jk_tasks.find(key);
-    if (it == P->jk_tasks.end()) {
-      auto t = std::make_unique<TaskSet>();
-      rc = build_jk_tasks(P, threshold, 0.0, *t);
-      if (rc) return rc;
-      CK(cudaStreamSynchronize(P->stream));
-      it = P->jk_tasks.emplace(key, std::move(t)).first;
-    }
-    ts = it->second.get();
+    ts = cached_tasks(P, threshold, 0.0, rc);
+    if (!ts) return rc;
   } else {
     if (!P->dense_tasks) {
       P->dense_tasks = std::make_unique<TaskSet>();
@@ -1559,15 +1572,9 @@ int igpu_grad_device(igpu_plan* P, const igpu_term* coulomb, int ncoul, const ig
   } else {
     CK(cudaStreamSynchronize(s));
   }
-  auto key = std::make_pair(threshold, fp64_cut);
-  auto it = P->jk_tasks.find(key);
-  if (it == P->jk_tasks.end()) {
-    auto ts = std::make_unique<TaskSet>();
-    int rc = build_jk_tasks(P, threshold, fp64_cut, *ts);
-    if (rc) return rc;
-    CK(cudaStreamSynchronize(P->stream));
-    it = P->jk_tasks.emplace(key, std::move(ts)).first;
-  }
+  int trc;
+  TaskSet* tasks = cached_tasks(P, threshold, fp64_cut, trc);
+  if (!tasks) return trc;
   KernelArgs A = base_args(P);
   A.mode = MODE_GRAD;
   const double* const* dp = P->d_gptr.p;
@@ -1587,7 +1594,7 @@ int igpu_grad_device(igpu_plan* P, const igpu_term* coulomb, int ncoul, const ig
   A.grad.out = d_out;
   A.bra_bitmap = bra_subset ? P->d_bitmap.p : nullptr;
   uint32_t launches = (uint32_t)mats.size();
-  int rc = run_tasks(P, *it->second, A, s, launches);
+  int rc = run_tasks(P, *tasks, A, s, launches);
   if (rc) return rc;
   CK(cudaStreamSynchronize(s));
   return collect_profile(P, 0, false, ncoul, nexch);
