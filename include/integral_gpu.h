@@ -105,6 +105,8 @@ typedef struct {
   uint64_t prim_quartets;
   double ms;                  /* device time (CUDA events) */
   double model_flops;         /* fixed Rys flop model of the accepted work */
+  uint32_t chunk;             /* tasks a warp claims per grab */
+  uint32_t reserved;
 } igpu_launch_record;
 
 /* integral-sys `integral_abi_version` (crates/integral-sys/src/lib.rs:21). */
@@ -241,6 +243,16 @@ int igpu_last_stats(const igpu_plan* plan, igpu_stats* stats);
 /* Per-launch records of the last J/K or gradient call (*n = count; at most
  * cap written to out). */
 int igpu_last_profile(const igpu_plan* plan, igpu_launch_record* out, size_t cap, size_t* n);
+/* Chunk autotuner for the J/K launches (no counterpart in the reference,
+ * whose CPU path has no launch shapes to tune).  Runs the J/K build of
+ * d_dens (device, ndens x nao x nao) at `threshold` and `precision` once
+ * per candidate chunk (4, 8, 16, 32 or 64 tasks per team per grab), twice
+ * over, into scratch outputs it allocates, and keeps per angular class and
+ * precision the chunk of the shortest launch.  Later J/K calls on the plan
+ * use the kept chunks (16 before any tuning); results differ only in the
+ * order of the atomic additions.  Costs ten J/K builds. */
+int igpu_autotune_jk(igpu_plan* plan, const double* d_dens, int ndens, double threshold, int precision,
+                     void* stream);
 
 #ifdef __cplusplus
 }

@@ -782,6 +782,13 @@ class DirectContractor:
             float(threshold), int(bool(want_exchange)), int(precision), ctypes.c_void_p(d_J),
             ctypes.c_void_p(d_K if want_exchange else 0), ctypes.c_void_p(stream or 0)))
 
+    def autotune_device(self, d_dens, ndens, threshold, precision: int = 1, stream=None):
+        """Chunk autotuner (igpu_autotune_jk; no reference counterpart): times
+        the J/K build of the device densities at candidate chunk sizes and
+        keeps the fastest per angular class and precision for later calls."""
+        _lib.check(_lib.lib().igpu_autotune_jk(self._plan.h, ctypes.c_void_p(d_dens), int(ndens), float(threshold),
+                                               int(precision), ctypes.c_void_p(stream or 0)))
+
     def set_mixed_cutoff(self, cutoff: float):
         """MIXED precision: quartets with Q_bra*Q_ket*max|D| below `cutoff`
         (default 1e-4) run in FP32 (igpu_set_mixed_cutoff)."""

@@ -36,7 +36,8 @@ class IgpuLaunchRecord(ctypes.Structure):
     _fields_ = [("la", ctypes.c_int), ("lb", ctypes.c_int), ("lc", ctypes.c_int), ("ld", ctypes.c_int),
                 ("fp32", ctypes.c_int), ("team", ctypes.c_int), ("grid", ctypes.c_uint32),
                 ("tasks", ctypes.c_uint64), ("quartets", ctypes.c_uint64), ("prim_quartets", ctypes.c_uint64),
-                ("ms", ctypes.c_double), ("model_flops", ctypes.c_double)]
+                ("ms", ctypes.c_double), ("model_flops", ctypes.c_double), ("chunk", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 STATUS = {
@@ -91,6 +92,7 @@ def lib():
                                    ctypes.c_int, c_u32_p, ctypes.c_size_t, ctypes.c_double, ctypes.c_int, vp, vp]
     L.igpu_last_stats.argtypes = [vp, ctypes.POINTER(IgpuStats)]
     L.igpu_last_profile.argtypes = [vp, ctypes.POINTER(IgpuLaunchRecord), ctypes.c_size_t, c_size_p]
+    L.igpu_autotune_jk.argtypes = [vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, vp]
     _lib = L
     return L
 
@@ -102,7 +104,7 @@ EXPORTED = [
     "igpu_eri_builder_fill", "igpu_eri_screened", "igpu_eri_block", "igpu_eri_packed", "igpu_plan_attach_aux", "igpu_aux_query", "igpu_schwarz_aux",
     "igpu_eri_2c", "igpu_eri_3c", "igpu_density_shell_bounds", "igpu_jk", "igpu_jk_device", "igpu_jk_device_static",
     "igpu_grad",
-    "igpu_grad_device", "igpu_last_stats", "igpu_last_profile",
+    "igpu_grad_device", "igpu_last_stats", "igpu_last_profile", "igpu_autotune_jk",
 ]
 
 

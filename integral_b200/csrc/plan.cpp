@@ -132,6 +132,10 @@ struct igpu_plan {
   // mixed-precision keys in insertion order: their cutoff follows max|D|,
   // so every new density would add one; at most kMixedTaskSets are kept
   std::vector<std::pair<double, double>> mixed_keys;
+  // chunk multiplier per J/K launch class (igpu_autotune_jk); tune_mult != 0
+  // overrides every launch while the tuner measures
+  std::map<int, int> tuned_mult;
+  int tune_mult = 0;
   std::unique_ptr<TaskSet> dense_tasks;
   double mixed_cutoff = 1e-4;
   double erf_omega = 0.0;  // 0: Coulomb; > 0: erf(omega r)/r for every later call
@@ -283,6 +287,9 @@ double model_flops_grad_quartet(int la, int lb, int lc, int ld, bool sph, int nt
   return f;
 }
 
+// Key of a J/K launch class in the tuned-chunk table.
+int tune_key(int pcb, int pck, bool fp32) { return (pcb * 64 + pck) * 2 + (fp32 ? 1 : 0); }
+
 // Scratch doubles per team: the class slot plus, for symmetric J/K, the
 // running bra-block accumulators (bra index + ndens blocks of the bra pair).
 size_t slot_with_acc(const KernelEntry* e, int pcb, const KernelArgs& A) {
@@ -326,7 +333,14 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     A.slot_doubles = slot_with_acc(e, L->pcb, A);
     A.acc_offset = e->slot;
     A.work_counter = P->d_work.p + li;
-    A.chunk = (unsigned long long)(32 / e->team) * 16;
+    int mult = 16;
+    if (P->tune_mult) {
+      mult = P->tune_mult;
+    } else if (A.mode == MODE_JK) {
+      auto t = P->tuned_mult.find(tune_key(L->pcb, L->pck, L->fp32));
+      if (t != P->tuned_mult.end()) mult = t->second;
+    }
+    A.chunk = (unsigned long long)(32 / e->team) * mult;
     if (A.counters) A.counters = P->d_launch_counters.p + li;
     A.task.bra_pair = L->bra_pair.p;
     A.task.ket_pairs = L->ket_list;
@@ -349,6 +363,7 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     r.team = e->team;
     r.grid = (uint32_t)grid;
     r.tasks = L->total;
+    r.chunk = (uint32_t)A.chunk;
     P->profile.push_back(r);
     P->profile_launch.push_back(li);
   }
@@ -888,6 +903,41 @@ int igpu_jk_device(igpu_plan* P, const double* d_dens, int ndens, const uint32_t
   }
   CK(cudaStreamSynchronize(s));
   return collect_profile(P, ndens, true);
+}
+
+int igpu_autotune_jk(igpu_plan* P, const double* d_dens, int ndens, double threshold, int precision, void* stream) {
+  if (!P || !d_dens) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (ndens < 1 || ndens > MAX_DENS) return fail(IGPU_ERR_DENSITY_COUNT, "1..64 densities");
+  const size_t n2 = (size_t)P->nao * P->nao * ndens;
+  DevBuf<double> tj, tk;
+  CK(tj.ensure(n2));
+  CK(tk.ensure(n2));
+  const int cand[] = {4, 8, 16, 32, 64};
+  std::map<int, std::map<int, float>> best;  // class key -> chunk -> shortest time
+  for (int rep = 0; rep < 2; ++rep)
+    for (int m : cand) {
+      P->tune_mult = m;
+      int rc = igpu_jk_device(P, d_dens, ndens, nullptr, 0, threshold, 1, precision, tj.p, tk.p, stream);
+      P->tune_mult = 0;
+      if (rc) return rc;
+      for (const igpu_launch_record& r : P->profile) {
+        const int key = tune_key(pair_class(r.la, r.lb), pair_class(r.lc, r.ld), r.fp32 != 0);
+        auto& slot = best[key];
+        auto it = slot.find(m);
+        if (it == slot.end() || r.ms < it->second) slot[m] = r.ms;
+      }
+    }
+  for (const auto& kv : best) {
+    int pick = 16;
+    float t = std::numeric_limits<float>::infinity();
+    for (const auto& mt : kv.second)
+      if (mt.second < t) {
+        t = mt.second;
+        pick = mt.first;
+      }
+    P->tuned_mult[kv.first] = pick;
+  }
+  return IGPU_OK;
 }
 
 int igpu_jk(igpu_plan* P, const double* dens, int ndens, const uint32_t* bra_subset, size_t nsub, double threshold,

@@ -59,6 +59,36 @@ def test_plan_create_validation_codes():
     assert b"NULL" in L.igpu_last_error_string()
 
 
+def test_ctypes_structs_match_the_header_layout(tmp_path):
+    """Every struct of include/integral_gpu.h, compiled by the host C
+    compiler, has the size and field offsets of its ctypes mirror."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    mirrors = {"igpu_shell": _lib.IgpuShell, "igpu_term": _lib.IgpuTerm, "igpu_stats": _lib.IgpuStats,
+               "igpu_launch_record": _lib.IgpuLaunchRecord}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "integral_gpu.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append('printf("%%s %%zu\\n", "%s", sizeof(%s));' % (cname, cname))
+        for f, _ in py._fields_:
+            lines.append('printf("%%s.%%s %%zu\\n", "%s", "%s", offsetof(%s, %s));' % (cname, f, cname, f))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                        text=True).stdout.splitlines())
+    for cname, py in mirrors.items():
+        assert int(got[cname]) == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert int(got["%s.%s" % (cname, f)]) == getattr(py, f).offset, (cname, f)
+    L = _lib.lib()
+    assert L.igpu_autotune_jk(None, None, 1, 0.0, 0, None) == -1
+
+
 def test_density_fitting_entries_reject_null_arguments():
     L = _lib.lib()
     assert L.igpu_plan_attach_aux(None, None, 0) == -1
