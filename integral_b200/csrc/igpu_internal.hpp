@@ -1,4 +1,4 @@
-// Internal data layout shared by the host plan (plan.cpp) and the device
+// Internal data layout shared by the host plan (plan*.cpp) and the device
 // kernels (kernels.cu).  Everything here is plain data in device memory.
 #pragma once
 #include <cstddef>

@@ -1,6 +1,6 @@
 // Registry of the per-class quartet kernels (compiled in class_tu.cu, one
 // module per bra pair class) and the small utility kernels (density
-// shell-block bounds, symmetry check).  The host plan (plan.cpp) calls only
+// shell-block bounds, symmetry check).  The host plan (plan*.cpp) calls only
 // the functions declared in launch.hpp.
 #include <cuda_runtime.h>
 

@@ -1,0 +1,192 @@
+// Internal header of the host plan: the plan object, its device buffers and
+// task lists, and the helpers that the C-ABI entry points share.  The entry
+// points are split by subsystem: plan.cpp (plan, Schwarz, launches,
+// profiles), plan_jk.cpp (direct J/K), plan_dense.cpp (dense tensor,
+// EriBuilder, screened tensor, blocks, packed tensor), plan_df.cpp (density
+// fitting) and plan_grad.cpp (the gradient).  Included by those files only.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/integral_gpu.h"
+#include "host_math.hpp"
+#include "launch.hpp"
+#include "noalloc.hpp"
+
+namespace igpu {
+namespace host {
+extern thread_local std::string g_err;
+
+inline int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+inline int cuda_fail(cudaError_t e, const char* where) {
+  g_err = std::string(where) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? IGPU_ERR_OUT_OF_MEMORY : IGPU_ERR_CUDA;
+}
+#define CK(expr)                                             \
+  do {                                                       \
+    cudaError_t _e = (expr);                                 \
+    if (_e != cudaSuccess) return cuda_fail(_e, #expr);      \
+  } while (0)
+
+inline int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
+inline int pc_la_host(int pc) {
+  int la = 0;
+  while ((la + 1) * (la + 2) / 2 <= pc) ++la;
+  return la;
+}
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t ensure(size_t count) {
+    if (count <= n && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+    if (e == cudaSuccess) n = std::max<size_t>(count, 1);
+    return e;
+  }
+  cudaError_t upload(const std::vector<T>& v, cudaStream_t s) {
+    cudaError_t e = ensure(v.size());
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+  }
+};
+
+// One class-pair launch of the quartet kernels.
+struct Launch {
+  int pcb = 0, pck = 0;
+  bool fp32 = false;
+  int builder_swap = 0;
+  int nbra = 0;
+  unsigned long long total = 0;
+  DevBuf<int> bra_pair, ket_start, own_kets;
+  DevBuf<unsigned long long> prefix;
+  const int* ket_list = nullptr;  // device Q-sorted pair list of the ket class
+};
+
+struct TaskSet {
+  std::vector<std::unique_ptr<Launch>> launches;
+};
+
+// Mixed-precision J/K task lists kept per plan (see igpu_plan::mixed_keys).
+constexpr size_t kMixedTaskSets = 4;
+
+}  // namespace host
+}  // namespace igpu
+
+
+// the plan's members name these types unqualified
+using namespace igpu;
+using namespace igpu::host;
+
+struct igpu_plan {
+  int device = 0;
+  int engine = 0;
+  int nsh = 0, nao = 0, natom = 0, npairs = 0;
+  bool spherical_any = false;
+  std::vector<DevShell> shells;
+  std::vector<std::array<double, 3>> atoms;
+  std::vector<PairD> pairs;            // canonical order p = tri(i, j)
+  std::vector<PrimPairD> prims;
+  std::vector<double> c2s;
+  int c2s_off[GPU_MAX_L + 3] = {0};
+  std::vector<std::vector<int>> class_pairs;  // per pair class: nprim desc, then Q desc
+  std::vector<std::vector<std::pair<size_t, size_t>>> class_groups;  // equal-nprim runs
+  std::vector<double> schwarz;               // nsh x nsh
+  // device
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  DevBuf<DevShell> d_shells;
+  DevBuf<PairD> d_pairs;
+  DevBuf<PrimPairD> d_prims;
+  DevBuf<double> d_c2s;
+  DevBuf<int> d_class_lists;
+  std::vector<int> class_list_off;
+  DevBuf<double> d_scratch;
+  DevBuf<Counters> d_counters;
+  DevBuf<double> d_schwarz_pair;
+  // per-call device buffers
+  DevBuf<double> d_D, d_J, d_K, d_bounds, d_dense, d_Jh, d_Kh;
+  DevBuf<unsigned long long> d_work;
+  DevBuf<unsigned long long> d_flag;
+  DevBuf<unsigned> d_bitmap;
+  std::map<std::pair<double, double>, std::unique_ptr<TaskSet>> jk_tasks;  // (threshold, fp64 cutoff)
+  // mixed-precision keys in insertion order: their cutoff follows max|D|,
+  // so every new density would add one; at most kMixedTaskSets are kept
+  std::vector<std::pair<double, double>> mixed_keys;
+  // chunk multiplier per J/K launch class (igpu_autotune_jk); tune_mult != 0
+  // overrides every launch while the tuner measures
+  std::map<int, int> tuned_mult;
+  int tune_mult = 0;
+  std::unique_ptr<TaskSet> dense_tasks;
+  double mixed_cutoff = 1e-4;
+  double erf_omega = 0.0;  // 0: Coulomb; > 0: erf(omega r)/r for every later call
+  bool all_spherical = false;
+  igpu_stats last{};
+  DevBuf<Counters> d_launch_counters;
+  std::vector<cudaEvent_t> events;
+  std::vector<igpu_launch_record> profile;
+  std::vector<size_t> profile_launch;
+  // gradient: term matrices, their block maxima and the device term tables
+  DevBuf<double> d_gmat, d_gmax, d_gfac, d_gout;
+  DevBuf<const double*> d_gptr;
+  // packed tensor: first AO-pair index of every canonical shell pair
+  DevBuf<long long> d_packed_start;
+  // density fitting: the auxiliary basis, attached after the main shells,
+  // pairs and primitive pairs (their counts stay nsh, npairs, nprims_main)
+  int nprims_main = 0;
+  bool has_aux = false;
+  int naux_sh = 0, naux = 0;
+  std::vector<std::vector<int>> aux_class_pairs;  // per aux pair class: nprim desc, then Q desc
+  std::vector<double> aux_q;                      // Schwarz factor per aux shell
+  DevBuf<int> d_aux_lists;
+  DevBuf<unsigned> d_fault;
+};
+
+namespace igpu {
+namespace host {
+
+// plan.cpp: the core every entry point shares
+int ensure_constants(int dev);
+size_t grid_for(const KernelEntry* e, bool fp32, unsigned long long total);
+KernelArgs base_args(igpu_plan* P);
+double model_flops_prim(int la, int lb, int lc, int ld);
+double model_flops_quartet(int la, int lb, int lc, int ld, bool sph, int ndens, bool jk);
+double model_flops_grad_prim(int la, int lb, int lc, int ld);
+double model_flops_grad_quartet(int la, int lb, int lc, int ld, bool sph, int nterm_c, int nterm_x);
+int tune_key(int pcb, int pck, bool fp32);
+size_t slot_with_acc(const KernelEntry* e, int pcb, const KernelArgs& A);
+int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t& launches);
+int collect_profile(igpu_plan* P, int ndens, bool jk, int grad_terms_c = -1, int grad_terms_x = 0);
+std::unique_ptr<Launch> make_launch(igpu_plan* P, int pcb, int pck, bool fp32, const std::vector<int>& bras,
+                                    const std::vector<int>& nket, const std::vector<int>& kstart,
+                                    const int* ket_list_dev, int swap, cudaStream_t s, int& rc);
+std::unique_ptr<Launch> owned_launch(igpu_plan* P, int pcb, int pck, const std::vector<int>& bras,
+                                     const std::vector<int>& nket, const std::vector<int>& kets, int& rc);
+int build_jk_tasks(igpu_plan* P, double tau, double fp64_cut, TaskSet& ts);
+TaskSet* cached_tasks(igpu_plan* P, double threshold, double fp64_cut, int& rc);
+int check_bra_subset(igpu_plan* P, const uint32_t* sub, size_t nsub, std::vector<unsigned>& bitmap);
+int run_schwarz(igpu_plan* P);
+
+}  // namespace host
+}  // namespace igpu
