@@ -201,7 +201,9 @@ int igpu_density_shell_bounds(const igpu_plan* plan, const double* dens, int nde
  * canonical bra pairs in bra_subset (NULL = all) in one launch sequence:
  * J[d] += sum (ab|cd) D[d]_cd, K[d] += sum (ab|cd) D[d]_bd over the
  * Schwarz/density-screened canonical quartets.  Host buffers; K may be NULL
- * when want_k == 0. */
+ * when want_k == 0.  The subset's indices must be distinct (a repeat is
+ * IGPU_ERR_INVALID_ARGUMENT: it would count once here, twice through
+ * per-bra calls); the gradient entries below follow the same rule. */
 int igpu_jk(igpu_plan* plan, const double* dens, int ndens, const uint32_t* bra_subset, size_t nsub,
             double threshold, int want_k, int precision, double* J, double* K);
 /* Same with device-resident D, J, K on a caller stream (cudaStream_t). */

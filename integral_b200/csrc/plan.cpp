@@ -389,11 +389,18 @@ TaskSet* cached_tasks(igpu_plan* P, double threshold, double fp64_cut, int& rc) 
   return out;
 }
 
-int check_bra_subset(igpu_plan* P, const uint32_t* sub, size_t nsub, std::vector<unsigned>& bitmap) {
+// Bitmap of a bra-pair subset.  Entry points that accumulate (J/K, the
+// gradient) pass accumulate = true: a repeated index would count once here
+// but twice through the reference's per-bra calls, so it is rejected.
+int check_bra_subset(igpu_plan* P, const uint32_t* sub, size_t nsub, std::vector<unsigned>& bitmap,
+                     bool accumulate) {
   bitmap.assign(((size_t)P->npairs + 31) / 32, 0u);
   for (size_t x = 0; x < nsub; ++x) {
     if (sub[x] >= (uint32_t)P->npairs) return fail(IGPU_ERR_NONCANONICAL_BRA, "bra pair index out of range");
-    bitmap[sub[x] / 32] |= 1u << (sub[x] % 32);
+    const unsigned bit = 1u << (sub[x] % 32);
+    if (accumulate && (bitmap[sub[x] / 32] & bit))
+      return fail(IGPU_ERR_INVALID_ARGUMENT, "bra pair " + std::to_string(sub[x]) + " repeated in the subset");
+    bitmap[sub[x] / 32] |= bit;
   }
   return IGPU_OK;
 }

@@ -165,7 +165,7 @@ int igpu_eri_packed(igpu_plan* P, double threshold, const uint32_t* sub, size_t 
   const size_t len = m * (m + 1) / 2;
   std::vector<unsigned> bitmap;
   if (sub) {
-    int rc = check_bra_subset(P, sub, nsub, bitmap);
+    int rc = check_bra_subset(P, sub, nsub, bitmap, false);
     if (rc) return rc;
   }
   cudaStream_t s = P->stream;

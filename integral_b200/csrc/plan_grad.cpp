@@ -29,7 +29,7 @@ int igpu_grad_device(igpu_plan* P, const igpu_term* coulomb, int ncoul, const ig
   cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
   std::vector<unsigned> bitmap;
   if (bra_subset) {
-    int rc = check_bra_subset(P, bra_subset, nsub, bitmap);
+    int rc = check_bra_subset(P, bra_subset, nsub, bitmap, true);
     if (rc) return rc;
     CK(P->d_bitmap.ensure(bitmap.size()));
     CK(cudaMemcpyAsync(P->d_bitmap.p, bitmap.data(), bitmap.size() * sizeof(unsigned), cudaMemcpyHostToDevice, s));

@@ -185,7 +185,8 @@ std::unique_ptr<Launch> owned_launch(igpu_plan* P, int pcb, int pck, const std::
                                      const std::vector<int>& nket, const std::vector<int>& kets, int& rc);
 int build_jk_tasks(igpu_plan* P, double tau, double fp64_cut, TaskSet& ts);
 TaskSet* cached_tasks(igpu_plan* P, double threshold, double fp64_cut, int& rc);
-int check_bra_subset(igpu_plan* P, const uint32_t* sub, size_t nsub, std::vector<unsigned>& bitmap);
+int check_bra_subset(igpu_plan* P, const uint32_t* sub, size_t nsub, std::vector<unsigned>& bitmap,
+                     bool accumulate);
 int run_schwarz(igpu_plan* P);
 
 }  // namespace host

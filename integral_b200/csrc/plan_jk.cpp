@@ -31,7 +31,7 @@ int igpu_jk_device(igpu_plan* P, const double* d_dens, int ndens, const uint32_t
   cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
   std::vector<unsigned> bitmap;
   if (bra_subset) {
-    int rc = check_bra_subset(P, bra_subset, nsub, bitmap);
+    int rc = check_bra_subset(P, bra_subset, nsub, bitmap, true);
     if (rc) return rc;
     CK(P->d_bitmap.ensure(bitmap.size()));
     CK(cudaMemcpyAsync(P->d_bitmap.p, bitmap.data(), bitmap.size() * sizeof(unsigned), cudaMemcpyHostToDevice, s));

@@ -64,3 +64,16 @@ def test_screening_error_is_bounded_on_extended_system():
         assert float(np.max(np.abs(screened - exact))) < 100.0 * thr
     nothing, st = contract(gc, coul, exch, float("inf"))
     assert st["quartets"] == 0 and np.all(nothing == 0.0)
+
+
+def test_repeated_bra_pair_is_rejected():
+    shells = S.direct_grad_fixture(False)
+    gc = contractor(shells)
+    coul, exch = S.grad_fixture_terms(O.OracleBasis(shells).nao)
+    with pytest.raises(ib.IntegralError) as e:
+        contract(gc, coul, exch, bras=[3, 5, 3])
+    assert e.value.code == -1
+    dc = ib.Basis(shells).direct_contractor()
+    D = S.grad_symmetric(O.OracleBasis(shells).nao, 2)[None]
+    with pytest.raises(ib.IntegralError):
+        dc.jk(D, 0.0, bras=[1, 1])
