@@ -211,7 +211,8 @@ int igpu_jk_device_static(igpu_plan* P, const double* d_dens, int ndens, double 
     A.slot_doubles = e->slot;
     A.acc_offset = e->slot;
     A.work_counter = sb.work + li;
-    A.chunk = (unsigned long long)(32 / e->team) * 16;
+    const auto tuned = P->tuned_mult.find(tune_key(L->pcb, L->pck, L->fp32));
+    A.chunk = (unsigned long long)(32 / e->team) * (tuned == P->tuned_mult.end() ? 16 : tuned->second);
     A.task.bra_pair = L->bra_pair.p;
     A.task.ket_pairs = L->ket_list;
     A.task.prefix = L->prefix.p;
