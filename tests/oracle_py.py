@@ -141,10 +141,7 @@ class OracleBasis:
         E = self.eri(engine)
         Q = self.schwarz(engine)
         n = self.nsh
-        keep = np.multiply.outer(Q, Q) >= tau  # [i, j, k, l]
-        nf = [(2 * s["l"] + 1) if s.get("spherical") else (s["l"] + 1) * (s["l"] + 2) // 2 for s in self.shells]
-        owner = np.repeat(np.arange(n), nf)
-        K = keep[np.ix_(owner, owner, owner, owner)]
+        K = self.screened_mask(tau, engine)
         pairs = [(i, j) for i in range(n) for j in range(i + 1)]
         total = skipped = 0
         for p, (i, j) in enumerate(pairs):
@@ -153,6 +150,15 @@ class OracleBasis:
                 if Q[i, j] * Q[k, l] < tau:
                     skipped += 1
         return np.where(K.reshape(-1), E, 0.0), total, skipped
+
+    def screened_mask(self, tau, engine="auto"):
+        """nao^4 boolean mask of the elements whose shell quartet passes
+        Q_ij*Q_kl >= tau (src/integrals.rs:905-909)."""
+        Q = self.schwarz(engine)
+        keep = np.multiply.outer(Q, Q) >= tau  # [i, j, k, l]
+        nf = [(2 * s["l"] + 1) if s.get("spherical") else (s["l"] + 1) * (s["l"] + 2) // 2 for s in self.shells]
+        owner = np.repeat(np.arange(self.nsh), nf)
+        return keep[np.ix_(owner, owner, owner, owner)]
 
     def eri_block(self, i, j, k, l, engine="auto"):
         nf = [(2 * s["l"] + 1) if s.get("spherical") else (s["l"] + 1) * (s["l"] + 2) // 2
