@@ -24,6 +24,13 @@ total work is fixed (strong scaling); time = max over ranks.
 `--impl reference` times the reference algorithm on the host cores: the C++
 restatement of the reference's CPU path (the Rust crate cannot be built in
 this image), all threads, each step a seeded sample of bra pairs.
+
+Other workloads (one JSON line each, 1 GPU):
+  --workload grad     density-direct ERI gradient, 100 atoms / nao 1400
+  --workload dense    dense 54^4 tensor of 6 atoms, HBM-write roofline
+  --workload jk-sph   J/K of 200 atoms / nao 5200 spherical f on every
+                      --sph-stride-th bra pair, with a full-build estimate
+  --profile-case      the small cases for ncu captures (no timing)
 """
 from __future__ import annotations
 
