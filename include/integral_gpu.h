@@ -255,6 +255,11 @@ int igpu_last_profile(const igpu_plan* plan, igpu_launch_record* out, size_t cap
  * order of the atomic additions.  Costs ten J/K builds. */
 int igpu_autotune_jk(igpu_plan* plan, const double* d_dens, int ndens, double threshold, int precision,
                      void* stream);
+/* The same chunk autotuner for the gradient launches: ten igpu_grad calls
+ * on the given (host) term matrices, at threshold and precision, into a
+ * scratch output; later gradient calls on the plan use the kept chunks. */
+int igpu_autotune_grad(igpu_plan* plan, const igpu_term* coulomb, int ncoul, const igpu_term* exchange,
+                       int nexch, double threshold, int precision);
 
 #ifdef __cplusplus
 }

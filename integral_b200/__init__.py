@@ -885,6 +885,15 @@ class DirectGradContractor:
             arr[k].right = r.ctypes.data_as(c_double_p)
         return arr, keep
 
+    def autotune(self, density: GradDensity, threshold: float, precision: int = 1):
+        """Chunk autotuner of the gradient launches (igpu_autotune_grad; no
+        reference counterpart): ten gradient builds of `density`; later
+        calls use the per-class chunks measured fastest."""
+        ca, k1 = self._terms(density.coulomb)
+        xa, k2 = self._terms(density.exchange)
+        _lib.check(_lib.lib().igpu_autotune_grad(self._plan.h, ca, len(density.coulomb), xa, len(density.exchange),
+                                                 float(threshold), int(precision)))
+
     def accumulate_bra_pairs(self, workspace, bra_indices, density: GradDensity, threshold: float, out: np.ndarray,
                              precision: int = 0, kernel: "EriKernel" = None):
         if density.nao != self._plan.nao:

@@ -93,6 +93,8 @@ def lib():
     L.igpu_last_stats.argtypes = [vp, ctypes.POINTER(IgpuStats)]
     L.igpu_last_profile.argtypes = [vp, ctypes.POINTER(IgpuLaunchRecord), ctypes.c_size_t, c_size_p]
     L.igpu_autotune_jk.argtypes = [vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, vp]
+    L.igpu_autotune_grad.argtypes = [vp, ctypes.POINTER(IgpuTerm), ctypes.c_int, ctypes.POINTER(IgpuTerm),
+                                     ctypes.c_int, ctypes.c_double, ctypes.c_int]
     _lib = L
     return L
 
@@ -104,7 +106,7 @@ EXPORTED = [
     "igpu_eri_builder_fill", "igpu_eri_screened", "igpu_eri_block", "igpu_eri_packed", "igpu_plan_attach_aux", "igpu_aux_query", "igpu_schwarz_aux",
     "igpu_eri_2c", "igpu_eri_3c", "igpu_density_shell_bounds", "igpu_jk", "igpu_jk_device", "igpu_jk_device_static",
     "igpu_grad",
-    "igpu_grad_device", "igpu_last_stats", "igpu_last_profile", "igpu_autotune_jk",
+    "igpu_grad_device", "igpu_last_stats", "igpu_last_profile", "igpu_autotune_jk", "igpu_autotune_grad",
 ]
 
 

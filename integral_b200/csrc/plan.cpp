@@ -142,8 +142,33 @@ double model_flops_grad_quartet(int la, int lb, int lc, int ld, bool sph, int nt
   return f;
 }
 
-// Key of a J/K launch class in the tuned-chunk table.
-int tune_key(int pcb, int pck, bool fp32) { return (pcb * 64 + pck) * 2 + (fp32 ? 1 : 0); }
+// Key of a launch class in the tuned-chunk table; gradient classes have
+// their own keys.
+int tune_key(int pcb, int pck, bool fp32, bool grad) {
+  return ((pcb * 64 + pck) * 2 + (fp32 ? 1 : 0)) | (grad ? (1 << 20) : 0);
+}
+
+// Chunk tuning: note every launch time of the last call made at chunk
+// multiplier m, then keep per class the multiplier of the shortest time.
+void tune_record(igpu_plan* P, int m, bool grad, std::map<int, std::map<int, float>>& best) {
+  for (const igpu_launch_record& r : P->profile) {
+    auto& slot = best[tune_key(pair_class(r.la, r.lb), pair_class(r.lc, r.ld), r.fp32 != 0, grad)];
+    auto it = slot.find(m);
+    if (it == slot.end() || r.ms < it->second) slot[m] = r.ms;
+  }
+}
+void tune_keep(igpu_plan* P, const std::map<int, std::map<int, float>>& best) {
+  for (const auto& kv : best) {
+    int pick = 16;
+    float t = std::numeric_limits<float>::infinity();
+    for (const auto& mt : kv.second)
+      if (mt.second < t) {
+        t = mt.second;
+        pick = mt.first;
+      }
+    P->tuned_mult[kv.first] = pick;
+  }
+}
 
 // Scratch doubles per team: the class slot plus, for symmetric J/K, the
 // running bra-block accumulators (bra index + ndens blocks of the bra pair).
@@ -191,8 +216,8 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     int mult = 16;
     if (P->tune_mult) {
       mult = P->tune_mult;
-    } else if (A.mode == MODE_JK) {
-      auto t = P->tuned_mult.find(tune_key(L->pcb, L->pck, L->fp32));
+    } else if (A.mode == MODE_JK || A.mode == MODE_GRAD) {
+      auto t = P->tuned_mult.find(tune_key(L->pcb, L->pck, L->fp32, A.mode == MODE_GRAD));
       if (t != P->tuned_mult.end()) mult = t->second;
     }
     A.chunk = (unsigned long long)(32 / e->team) * mult;

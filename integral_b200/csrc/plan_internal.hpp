@@ -134,7 +134,8 @@ struct igpu_plan {
   // mixed-precision keys in insertion order: their cutoff follows max|D|,
   // so every new density would add one; at most kMixedTaskSets are kept
   std::vector<std::pair<double, double>> mixed_keys;
-  // chunk multiplier per J/K launch class (igpu_autotune_jk); tune_mult != 0
+  // chunk multiplier per J/K or gradient launch class (igpu_autotune_jk,
+  // igpu_autotune_grad); tune_mult != 0
   // overrides every launch while the tuner measures
   std::map<int, int> tuned_mult;
   int tune_mult = 0;
@@ -174,7 +175,9 @@ double model_flops_prim(int la, int lb, int lc, int ld);
 double model_flops_quartet(int la, int lb, int lc, int ld, bool sph, int ndens, bool jk);
 double model_flops_grad_prim(int la, int lb, int lc, int ld);
 double model_flops_grad_quartet(int la, int lb, int lc, int ld, bool sph, int nterm_c, int nterm_x);
-int tune_key(int pcb, int pck, bool fp32);
+int tune_key(int pcb, int pck, bool fp32, bool grad);
+void tune_record(igpu_plan* P, int m, bool grad, std::map<int, std::map<int, float>>& best);
+void tune_keep(igpu_plan* P, const std::map<int, std::map<int, float>>& best);
 size_t slot_with_acc(const KernelEntry* e, int pcb, const KernelArgs& A);
 int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t& launches);
 int collect_profile(igpu_plan* P, int ndens, bool jk, int grad_terms_c = -1, int grad_terms_x = 0);

@@ -111,23 +111,9 @@ int igpu_autotune_jk(igpu_plan* P, const double* d_dens, int ndens, double thres
       int rc = igpu_jk_device(P, d_dens, ndens, nullptr, 0, threshold, 1, precision, tj.p, tk.p, stream);
       P->tune_mult = 0;
       if (rc) return rc;
-      for (const igpu_launch_record& r : P->profile) {
-        const int key = tune_key(pair_class(r.la, r.lb), pair_class(r.lc, r.ld), r.fp32 != 0);
-        auto& slot = best[key];
-        auto it = slot.find(m);
-        if (it == slot.end() || r.ms < it->second) slot[m] = r.ms;
-      }
+      tune_record(P, m, false, best);
     }
-  for (const auto& kv : best) {
-    int pick = 16;
-    float t = std::numeric_limits<float>::infinity();
-    for (const auto& mt : kv.second)
-      if (mt.second < t) {
-        t = mt.second;
-        pick = mt.first;
-      }
-    P->tuned_mult[kv.first] = pick;
-  }
+  tune_keep(P, best);
   return IGPU_OK;
 }
 
@@ -211,7 +197,7 @@ int igpu_jk_device_static(igpu_plan* P, const double* d_dens, int ndens, double 
     A.slot_doubles = e->slot;
     A.acc_offset = e->slot;
     A.work_counter = sb.work + li;
-    const auto tuned = P->tuned_mult.find(tune_key(L->pcb, L->pck, L->fp32));
+    const auto tuned = P->tuned_mult.find(tune_key(L->pcb, L->pck, L->fp32, false));
     A.chunk = (unsigned long long)(32 / e->team) * (tuned == P->tuned_mult.end() ? 16 : tuned->second);
     A.task.bra_pair = L->bra_pair.p;
     A.task.ket_pairs = L->ket_list;

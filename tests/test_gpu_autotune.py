@@ -1,7 +1,7 @@
-"""The J/K chunk autotuner (igpu_autotune_jk): after tuning, every J/K
-launch runs with a chunk from the candidate set, and J and K equal the
-untuned build within 1e-12 of their maxima (only the order of the atomic
-additions changes)."""
+"""The chunk autotuners (igpu_autotune_jk, igpu_autotune_grad): after
+tuning, every launch runs with a chunk from the candidate set, and J, K and
+the gradient equal the untuned builds within 1e-12 of their maxima (only
+the order of the atomic additions changes)."""
 import numpy as np
 import pytest
 
@@ -30,3 +30,17 @@ def test_autotune_keeps_results_and_sets_candidate_chunks():
     for a, b in ((J0, J1), (K0, K1)):
         a, b = a.cpu().numpy(), b.cpu().numpy()
         assert float(np.max(np.abs(a - b))) < 1e-12 * float(np.max(np.abs(a)))
+
+
+def test_gradient_autotune_keeps_results():
+    shells = S.direct_grad_fixture(True)
+    gc = ib.Basis(shells).direct_grad_contractor()
+    n = gc.nao()
+    coul, exch = S.grad_fixture_terms(n)
+    dens = gc.density([ib.GradDensityTerm(*t) for t in coul], [ib.GradDensityTerm(*t) for t in exch])
+    g0 = gc.contract(dens, threshold=0.0, precision=1)
+    gc.autotune(dens, 0.0, 1)
+    g1 = gc.contract(dens, threshold=0.0, precision=1)
+    for r in gc._plan.profile():
+        assert r["chunk"] // (32 // r["team"]) in (4, 8, 16, 32, 64)
+    assert float(np.max(np.abs(g0 - g1))) < 1e-12 * float(np.max(np.abs(g0)))
