@@ -270,6 +270,11 @@ class Basis:
         self._shells = [s if isinstance(s, Shell) else Shell.from_dict(s) for s in shells]
         self._plans = {}
 
+    @classmethod
+    def new(cls, shells: Sequence[Shell]) -> "Basis":
+        """Basis::new (src/shell.rs)."""
+        return cls(shells)
+
     def shells(self):
         return list(self._shells)
 
