@@ -99,6 +99,7 @@ def grad_bench(args):
     dens = gc.density([ib.GradDensityTerm(f, l, r) for f, l, r in s["coulomb"]],
                       [ib.GradDensityTerm(f, l, r) for f, l, r in s["exchange"]])
     bras = np.arange(0, len(gc.bra_pairs()), args.grad_stride)
+    nmat = len({id(m) for _, l, r in s["coulomb"] + s["exchange"] for m in (l, r)})
 
     def run(prec):
         out = np.zeros((gc.natom(), 3))
@@ -135,7 +136,10 @@ def grad_bench(args):
         "model_tflops": f32 / (ms32 * 1e-3) / 1e12,
         "max_abs_mixed_minus_fp64": float(np.abs(g32 - g64).max()),
         "max_abs_gradient": float(np.abs(g64).max()),
-        "e2e": {"value": q32 / w32, "unit": "quartets/s"},
+        "e2e": {"value": q32 / w32, "unit": "quartets/s",
+                # the distinct term matrices go up once per call, the natom x 3 gradient comes back
+                "h2d_bytes_per_step": int(8 * nmat * S.nao_of(s["shells"]) ** 2),
+                "d2h_bytes_per_step": int(8 * 3 * gc.natom())},
     }
     print(json.dumps(line))
 
