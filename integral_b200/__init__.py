@@ -12,6 +12,15 @@ reference (Rust)           here
                            ``schwarz_bounds``, ``direct_contractor``, ...)
 ``Engine``                 :class:`Engine` (src/integrals.rs:329-338)
 ``EriBuilder``             :class:`EriBuilder` (src/eri_builder.rs)
+``PackedEriBuilder``       :class:`PackedEriBuilder`, :class:`PackedBraFill`,
+                           :class:`PackedEriWorkspace` (src/packed_eri.rs)
+``Eri3cBuilder``           :class:`Eri3cBuilder`, :class:`Bra3cFill`;
+                           ``Basis.eri_2c``, ``Basis.schwarz_aux_bounds``
+                           (src/df.rs)
+``EriKernel``              :class:`EriKernel` (``Coulomb``, ``Erf(omega)``;
+                           src/integrals.rs:304-321)
+``ScreeningStats``         :class:`ScreeningStats` (src/integrals.rs:983-1005)
+``select_engine``          :func:`select_engine` (src/integrals.rs:374-388)
 ``DirectContractor``       :class:`DirectContractor`, :class:`DirectWorkspace`,
                            :class:`DirectBuffers` (src/direct.rs)
 ``DirectGradContractor``   :class:`DirectGradContractor`,
