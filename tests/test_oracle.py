@@ -547,3 +547,20 @@ def test_select_engine_policy_matches_the_oracle():
             for deg in (1, 2, 3, 4, 15, 16, 17, 81, 256):
                 want = {"os": ib.Engine.OsHgp, "rys": ib.Engine.Rys}[O.select_engine(ne, nf, deg)]
                 assert ib.select_engine(ne, nf, deg) == want, (ne, nf, deg)
+
+
+def test_df_erf_metric_concentric_s_closed_form():
+    # tests/erf_kernel.rs:428-481 (2c/3c through the unit-s dummy under
+    # erf): two concentric s functions have T = 0, so
+    # (P|Q)_erf = N_a N_b 2 pi^(5/2) / (a b sqrt(a+b)) * sqrt(s),
+    # s = omega^2 / (rho + omega^2), rho = a b / (a + b)
+    a, b, omega = 0.9, 1.7, 0.6
+    aux = [dict(l=0, spherical=False, center=[0.0] * 3, exps=[a], coefs=[1.0]),
+           dict(l=0, spherical=False, center=[0.0] * 3, exps=[b], coefs=[1.0])]
+    with O.erf(omega):
+        m = O.df_eri_2c(aux, "rys")
+    rho = a * b / (a + b)
+    sc = omega ** 2 / (rho + omega ** 2)
+    want = _s_norm(a) * _s_norm(b) * 2.0 * np.pi ** 2.5 / (a * b * np.sqrt(a + b)) * np.sqrt(sc)
+    _close(m[1], want, 1e-12)
+    assert m[1] == m[2]
