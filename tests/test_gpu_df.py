@@ -109,3 +109,16 @@ def test_erf_metric_and_3c_match_oracle():
     check(main.eri_3c_block_kernel(aux, 3, 1, 2, k), ref3)
     # Coulomb again afterwards
     check(aux.eri_2c(), O.df_eri_2c(a))
+
+
+def test_erf_metric_concentric_s_closed_form():
+    # two concentric s functions under erf(omega r)/r: the Coulomb closed
+    # form times sqrt(omega^2 / (rho + omega^2)) (tests/df.rs:53-68 with the
+    # attenuation of src/engine/rys.rs:163-175)
+    a, b, omega = 0.9, 1.7, 0.6
+    aux = ib.Basis([ib.Shell.new(0, [0.0, 0.0, 0.0], [a], [1.0]), ib.Shell.new(0, [0.0, 0.0, 0.0], [b], [1.0])])
+    m = aux.eri_2c_kernel(ib.EriKernel.Erf(omega))
+    norm = lambda x: (2.0 * x / np.pi) ** 0.75
+    rho = a * b / (a + b)
+    want = norm(a) * norm(b) * 2.0 * np.pi ** 2.5 / (a * b * np.sqrt(a + b)) * np.sqrt(omega ** 2 / (rho + omega ** 2))
+    assert abs(m[1] - want) < 1e-12 * want and m[1] == m[2]
