@@ -128,8 +128,21 @@ int igpu_plan_query(const igpu_plan* plan, size_t* nao, size_t* natom, size_t* n
 int igpu_bra_pairs(const igpu_plan* plan, uint32_t* pairs);
 /* Basis::atoms (shell.rs:250-258): natom x 3 centres. */
 int igpu_atoms(const igpu_plan* plan, double* xyz);
-/* Basis::schwarz_bounds (integrals.rs:835-862): nsh x nsh, row-major. */
+/* Basis::schwarz_bounds (integrals.rs:835-862): nsh x nsh, row-major.
+ * Wherever the reference's Auto policy (integrals.rs:374-388) evaluates a
+ * diagonal quartet with OS/HGP, which covers every shell pair of a basis of
+ * contracted shells, the plan holds the host's bit-exact evaluation of it,
+ * so the screened quartet lists equal the reference's by construction; the
+ * other pairs (see igpu_schwarz_bounds) keep the device's Rys evaluation. */
 int igpu_schwarz(const igpu_plan* plan, double* q);
+/* Basis::schwarz_bounds of a shell list on the host, without a device or a
+ * plan: the same bit-exact bounds, nsh x nsh row-major.  An ordered shell
+ * pair whose diagonal quartet the Auto policy sends to the Rys engine (one
+ * primitive on each shell at l_i + l_j >= 3, fewer than four primitive pairs
+ * at l_i + l_j >= 7, or l_i + l_j > 8) has no host evaluation: its entry is
+ * NaN and it is counted in *n_rys (n_rys may be NULL).  A plan holds the
+ * device evaluation for those pairs (within 1e-14 of the reference). */
+int igpu_schwarz_bounds(const igpu_shell* shells, size_t nsh, double* q, size_t* n_rys);
 /* Plan cutoff for IGPU_PRECISION_MIXED (default 1e-4). */
 int igpu_set_mixed_cutoff(igpu_plan* plan, double cutoff);
 /* EriKernel (src/integrals.rs:304-321) of every later call on the plan:
@@ -226,7 +239,10 @@ int igpu_jk_device(igpu_plan* plan, const double* d_dens, int ndens, const uint3
  * arrays, so calls that overlap on the GPU race: order them on one stream.
  * Also needs the FP64 task list of `threshold`, built by one earlier
  * igpu_jk or igpu_jk_device call on this plan with the same threshold.
- * Does not update igpu_last_stats / igpu_last_profile. */
+ * The plan's device must be the current device.  With a caller stream the
+ * call only queues its work on that stream (read J/K after synchronising
+ * it); with stream == NULL it runs on the plan's stream and returns when
+ * the work is done.  Does not update igpu_last_stats / igpu_last_profile. */
 int igpu_jk_device_static(igpu_plan* plan, const double* d_dens, int ndens, double threshold, int want_k,
                           double* d_J, double* d_K, void* stream);
 

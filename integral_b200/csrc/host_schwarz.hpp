@@ -1,0 +1,36 @@
+// Exact Schwarz bounds on the host (host_schwarz.cpp): the diagonal quartets
+// (ij|ij) evaluated with the reference's arithmetic, bit for bit, wherever its
+// Auto engine policy picks Obara-Saika / Head-Gordon-Pople.
+#pragma once
+#include <utility>
+#include <vector>
+
+namespace igpu {
+
+// One shell as the reference engine sees it: raw exponents, effective
+// coefficients (src/shell.rs:182-187) and, for a spherical shell, its
+// (2l+1) x n_cart transform with the normalisation ratio folded in
+// (src/spherical.rs:37-48); c2s == nullptr for a Cartesian shell.
+struct SchwarzShell {
+  int l = 0;
+  double center[3] = {0.0, 0.0, 0.0};
+  std::vector<double> exps, coefs;
+  const double* c2s = nullptr;
+};
+
+// src/integrals.rs:374-388: does Auto pick OS/HGP for bra degree ne, ket
+// degree nf and contraction degree `degree` (the product of the four raw
+// primitive counts)?
+bool auto_picks_os(int ne, int nf, long long degree);
+
+// Q = sqrt(max |(mu nu|mu nu)|) of shells (si, sj) in that order
+// (src/integrals.rs:850-860).  Returns false, leaving q untouched, when
+// Auto picks the Rys engine for the quartet.
+bool schwarz_exact(const SchwarzShell& si, const SchwarzShell& sj, double& q);
+
+// schwarz_exact over a list of ordered shell pairs on `nthreads` host
+// threads (<= 0: all hardware threads); done[x] = 1 where q[x] was set.
+void schwarz_exact_many(const std::vector<SchwarzShell>& shells, const std::vector<std::pair<int, int>>& pairs,
+                        std::vector<double>& q, std::vector<unsigned char>& done, int nthreads);
+
+}  // namespace igpu

@@ -57,14 +57,24 @@ int ensure_constants(int dev) {
   return IGPU_OK;
 }
 
-size_t grid_for(const KernelEntry* e, bool fp32, unsigned long long total) {
-  static int nsm = 0;
-  if (!nsm) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (nsm <= 0) nsm = 1;
+// SM count of the current device, looked up once per device.
+static int sm_count() {
+  static std::mutex m;
+  static std::vector<int> count;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(m);
+  if ((int)count.size() <= dev) count.resize(dev + 1, 0);
+  if (!count[dev]) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    count[dev] = n > 0 ? n : 1;
   }
+  return count[dev];
+}
+
+size_t grid_for(const KernelEntry* e, bool fp32, unsigned long long total) {
+  const int nsm = sm_count();
   const int teams_per_block = 128 / e->team;
   const unsigned long long need = (total + teams_per_block - 1) / teams_per_block;
   const unsigned long long cap = (unsigned long long)blocks_per_sm(e, fp32) * nsm;
@@ -388,9 +398,10 @@ int build_jk_tasks(igpu_plan* P, double tau, double fp64_cut, TaskSet& ts) {
 // The task list of (threshold, fp64 cutoff), built on first use and cached.
 // A mixed list's cutoff follows the maximum of the density (or term
 // matrices), so only the kMixedTaskSets most recent mixed lists are kept;
-// FP64 lists (cutoff 0, one per threshold) stay.  Every entry point
-// synchronises before it returns, so an evicted list has no launch in
-// flight.
+// FP64 lists (cutoff 0, one per threshold) stay.  Every entry point that
+// builds or evicts a list synchronises before it returns, so an evicted
+// list has no launch in flight; igpu_jk_device_static only reads FP64
+// lists, which are never evicted.
 TaskSet* cached_tasks(igpu_plan* P, double threshold, double fp64_cut, int& rc) {
   rc = IGPU_OK;
   const auto key = std::make_pair(threshold, fp64_cut);
@@ -464,6 +475,27 @@ int run_schwarz(igpu_plan* P) {
     P->schwarz[(size_t)j * P->nsh + i] = q[p];
   }
   return IGPU_OK;
+}
+
+// Replace the device Q of every canonical pair for which the reference's
+// Auto policy picks OS/HGP by the host's bit-exact evaluation in the
+// reference orientation (shell i, shell j), so that every threshold
+// comparison of the screening is the reference's.
+void exact_schwarz(igpu_plan* P) {
+  std::vector<std::pair<int, int>> ij(P->npairs);
+  for (int p = 0; p < P->npairs; ++p) ij[p] = {P->pairs[p].i, P->pairs[p].j};
+  std::vector<double> q;
+  std::vector<unsigned char> done;
+  schwarz_exact_many(P->sshells, ij, q, done, 0);
+  P->schwarz_exact_pairs = 0;
+  for (int p = 0; p < P->npairs; ++p) {
+    if (!done[p]) continue;
+    ++P->schwarz_exact_pairs;
+    P->pairs[p].q = q[p];
+    const int i = P->pairs[p].i, j = P->pairs[p].j;
+    P->schwarz[(size_t)i * P->nsh + j] = q[p];
+    P->schwarz[(size_t)j * P->nsh + i] = q[p];
+  }
 }
 
 // One launch whose ket list is owned by the launch: bra b runs kets
@@ -544,6 +576,14 @@ int igpu_plan_create(const igpu_shell* sh, size_t nsh, int engine, igpu_plan** o
       P->atoms.push_back({d.cx, d.cy, d.cz});
     }
     d.atom = atom;
+    SchwarzShell ss;
+    ss.l = d.l;
+    ss.center[0] = d.cx;
+    ss.center[1] = d.cy;
+    ss.center[2] = d.cz;
+    ss.exps.assign(expv.end() - d.nprim, expv.end());
+    ss.coefs.assign(eff.end() - d.nprim, eff.end());
+    P->sshells.push_back(std::move(ss));
     if (d.spherical) P->spherical_any = true;
     P->all_spherical = (s == 0 ? true : P->all_spherical) && d.spherical;
     P->shells.push_back(d);
@@ -562,6 +602,8 @@ int igpu_plan_create(const igpu_shell* sh, size_t nsh, int engine, igpu_plan** o
     P->c2s.insert(P->c2s.end(), m.begin(), m.end());
   }
   P->c2s_off[GPU_MAX_L + 2] = (int)P->c2s.size();
+  for (int s = 0; s < (int)nsh; ++s)
+    if (P->shells[s].spherical) P->sshells[s].c2s = P->c2s.data() + P->c2s_off[P->shells[s].l];
   // canonical pairs (integrals.rs:1252-1260) and primitive-pair data in
   // evaluation orientation (l_a >= l_b), screened as os_eri.rs:211-244
   const int npc = pair_class(lmax, lmax) + 1;
@@ -631,6 +673,7 @@ int igpu_plan_create(const igpu_shell* sh, size_t nsh, int engine, igpu_plan** o
   }
   rc = run_schwarz(P.get());
   if (rc) return rc;
+  exact_schwarz(P.get());
   // re-sort every class by (primitive-pair count desc, Q desc, index) and
   // record the equal-count groups used to cut task segments
   {
@@ -696,9 +739,62 @@ int igpu_atoms(const igpu_plan* P, double* xyz) {
   return IGPU_OK;
 }
 
-int igpu_schwarz(const igpu_plan* P, double* q) {
-  if (!P || !q) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+int igpu_schwarz(const igpu_plan* Pc, double* q) {
+  if (!Pc || !q) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  igpu_plan* P = const_cast<igpu_plan*>(Pc);
+  if (!P->schwarz_upper_done) {
+    // Q[j][i], j < i, is the reference's own evaluation of (j i|j i) (it
+    // computes every ordered pair), which may differ from Q[i][j] in the
+    // last bit
+    std::vector<std::pair<int, int>> ji;
+    for (int p = 0; p < P->npairs; ++p)
+      if (P->pairs[p].i != P->pairs[p].j) ji.push_back({P->pairs[p].j, P->pairs[p].i});
+    std::vector<double> v;
+    std::vector<unsigned char> done;
+    schwarz_exact_many(P->sshells, ji, v, done, 0);
+    for (size_t x = 0; x < ji.size(); ++x)
+      if (done[x]) P->schwarz[(size_t)ji[x].first * P->nsh + ji[x].second] = v[x];
+    P->schwarz_upper_done = true;
+  }
   std::memcpy(q, P->schwarz.data(), P->schwarz.size() * sizeof(double));
+  return IGPU_OK;
+}
+
+int igpu_schwarz_bounds(const igpu_shell* sh, size_t nsh, double* q, size_t* n_rys) {
+  if (nsh > 0 && (!sh || !q)) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (n_rys) *n_rys = 0;
+  std::vector<SchwarzShell> ss(nsh);
+  for (size_t s = 0; s < nsh; ++s) {
+    // validation order of Shell::with_kind (src/shell.rs:92-118)
+    if (sh[s].nprim <= 0) return fail(IGPU_ERR_EMPTY_CONTRACTION, "shell has no primitives");
+    if (!sh[s].exps || !sh[s].coefs) return fail(IGPU_ERR_INVALID_ARGUMENT, "shell exponents/coefficients NULL");
+    if (sh[s].l < 0) return fail(IGPU_ERR_INVALID_ARGUMENT, "negative angular momentum");
+    if (sh[s].l > MAX_L) return fail(IGPU_ERR_ANGULAR_MOMENTUM, "angular momentum exceeds supported maximum 6");
+    ss[s].l = sh[s].l;
+    for (int c = 0; c < 3; ++c) ss[s].center[c] = sh[s].center[c];
+    for (int p = 0; p < sh[s].nprim; ++p) {
+      ss[s].exps.push_back(sh[s].exps[p]);
+      ss[s].coefs.push_back(effective_coeff(sh[s].exps[p], sh[s].coefs[p], sh[s].l));
+    }
+  }
+  std::vector<std::vector<double>> mats(MAX_L + 1);
+  for (size_t s = 0; s < nsh; ++s)
+    if (sh[s].spherical) {
+      if (mats[sh[s].l].empty()) mats[sh[s].l] = c2s_effective(sh[s].l);
+      ss[s].c2s = mats[sh[s].l].data();
+    }
+  std::vector<std::pair<int, int>> all;
+  for (int i = 0; i < (int)nsh; ++i)
+    for (int j = 0; j < (int)nsh; ++j) all.push_back({i, j});
+  std::vector<double> v;
+  std::vector<unsigned char> done;
+  schwarz_exact_many(ss, all, v, done, 0);
+  size_t rys = 0;
+  for (size_t x = 0; x < all.size(); ++x) {
+    q[x] = done[x] ? v[x] : std::numeric_limits<double>::quiet_NaN();
+    rys += done[x] ? 0 : 1;
+  }
+  if (n_rys) *n_rys = rys;
   return IGPU_OK;
 }
 

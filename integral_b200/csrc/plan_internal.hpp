@@ -21,6 +21,7 @@
 
 #include "../../include/integral_gpu.h"
 #include "host_math.hpp"
+#include "host_schwarz.hpp"
 #include "launch.hpp"
 #include "noalloc.hpp"
 
@@ -113,6 +114,11 @@ struct igpu_plan {
   std::vector<std::vector<int>> class_pairs;  // per pair class: nprim desc, then Q desc
   std::vector<std::vector<std::pair<size_t, size_t>>> class_groups;  // equal-nprim runs
   std::vector<double> schwarz;               // nsh x nsh
+  // the shells as the host Schwarz evaluation sees them; the upper triangle
+  // Q[j][i] (j < i) is evaluated on the first igpu_schwarz call
+  std::vector<SchwarzShell> sshells;
+  size_t schwarz_exact_pairs = 0;  // canonical pairs whose Q is the host's exact value
+  bool schwarz_upper_done = false;
   // device
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -191,6 +197,7 @@ TaskSet* cached_tasks(igpu_plan* P, double threshold, double fp64_cut, int& rc);
 int check_bra_subset(igpu_plan* P, const uint32_t* sub, size_t nsub, std::vector<unsigned>& bitmap,
                      bool accumulate);
 int run_schwarz(igpu_plan* P);
+void exact_schwarz(igpu_plan* P);
 
 }  // namespace host
 }  // namespace igpu
