@@ -154,6 +154,13 @@ int igpu_jk_device_static(igpu_plan* P, const double* d_dens, int ndens, double 
   if (it == P->jk_tasks.end())
     return fail(IGPU_ERR_INVALID_ARGUMENT,
                 "no FP64 task list for this threshold: call igpu_jk or igpu_jk_device with it once first");
+  // the plan's buffers live on P->device; the static arrays are looked up
+  // on the current device, so the two must agree
+  int cur_dev = -1;
+  CK(cudaGetDevice(&cur_dev));
+  if (cur_dev != P->device)
+    return fail(IGPU_ERR_INVALID_ARGUMENT, "current device " + std::to_string(cur_dev) +
+                                               " is not the plan's device " + std::to_string(P->device));
   StaticBufs sb;
   CK(static_buffers(&sb));
   const size_t nb = (size_t)ndens * P->nsh * P->nsh;
@@ -209,6 +216,10 @@ int igpu_jk_device_static(igpu_plan* P, const double* d_dens, int ndens, double 
     A.builder_swap = 0;
     CK(launch_quartets(e, false, (int)grid, A, s));
   }
+  // on the plan's private stream the caller has nothing to wait on: finish
+  // here, as the other entry points do; on a caller stream the work stays
+  // queued there
+  if (!stream) CK(cudaStreamSynchronize(s));
   return IGPU_OK;
 }
 

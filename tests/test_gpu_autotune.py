@@ -8,7 +8,7 @@ import pytest
 import integral_b200 as ib
 from integral_b200 import systems as S
 
-pytestmark = [pytest.mark.gpu, pytest.mark.skip(reason="pending its first run on a B200")]
+pytestmark = pytest.mark.gpu
 
 
 def test_autotune_keeps_results_and_sets_candidate_chunks():

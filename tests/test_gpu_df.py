@@ -15,7 +15,7 @@ import integral_b200 as ib
 import oracle_py as O
 from integral_b200 import systems as S
 
-pytestmark = [pytest.mark.gpu, pytest.mark.skip(reason="density-fitting path: pending its first run on a B200")]
+pytestmark = pytest.mark.gpu
 
 
 def check(gpu, ref):

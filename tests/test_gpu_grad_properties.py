@@ -11,7 +11,7 @@ import integral_b200 as ib
 import oracle_py as O
 from integral_b200 import systems as S
 
-pytestmark = [pytest.mark.gpu, pytest.mark.skip(reason="pending its first run on a B200")]
+pytestmark = pytest.mark.gpu
 
 
 def contractor(shells):

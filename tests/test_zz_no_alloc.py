@@ -35,13 +35,20 @@ def test_static_entry_matches_allocating_entry_on_two_calls_in_a_row():
     K0 = torch.zeros_like(D)
     dc.jk_device(D.data_ptr(), 2, J0.data_ptr(), K0.data_ptr(), thr)
     torch.cuda.synchronize()
-    for _ in range(2):
-        J = torch.zeros_like(D)
-        K = torch.zeros_like(D)
+    outs = [(torch.zeros_like(D), torch.zeros_like(D)) for _ in range(2)]
+    # the first static call does the per-device set-up; the ones after it
+    # must leave the device's free memory exactly where it was
+    free_before = None
+    for J, K in outs:
         dc.jk_device_static(D.data_ptr(), 2, J.data_ptr(), K.data_ptr(), thr)
         torch.cuda.synchronize()
+        free_after = torch.cuda.mem_get_info()[0]
+        if free_before is not None:
+            assert free_after == free_before
+        free_before = free_after
         assert rel(J, J0) < 1e-12
         assert rel(K, K0) < 1e-12
+    J, K = outs[-1]
     # outputs accumulate
     dc.jk_device_static(D.data_ptr(), 2, J.data_ptr(), K.data_ptr(), thr)
     torch.cuda.synchronize()
