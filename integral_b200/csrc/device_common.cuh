@@ -311,6 +311,54 @@ __device__ __forceinline__ QuartetHdr<R> quartet_header(const PrimPairD& bp, con
   return h;
 }
 
+// The Rys parameter T of a primitive quartet in FP64 from the double pair
+// data (the same expression as quartet_header, erf scaling included).
+__device__ __forceinline__ double quartet_T64(const PrimPairD& bp, const PrimPairD& kp, double omega) {
+  const double p = bp.zeta, q = kp.zeta, pq = p + q;
+  const double rho = p * q / pq;
+  const double dx = bp.px - kp.px, dy = bp.py - kp.py, dz = bp.pz - kp.pz;
+  double T = rho * (dx * dx + dy * dy + dz * dz);
+  if (omega > 0.0) T *= omega * omega / (rho + omega * omega);
+  return T;
+}
+
+// Root r of the N-point quadrature at T, evaluated in FP64 from the double
+// tables (the FP32 launches take this path for large T and high l).
+template <int N>
+__device__ __forceinline__ void rys_root_fp64(double T, int r, double& x, double& w) {
+  const RysMeta m = c_rys[N];
+  if (T >= m.t_hi) {
+    x = c_lag_x[N - 1][r] / T;
+    w = c_lag_w[N - 1][r] * 0.5 * rsqrt(T);
+    return;
+  }
+  int s = (int)(T / m.width);
+  s = s < 0 ? 0 : (s >= m.n_sub ? m.n_sub - 1 : s);
+  const double a = (double)s * m.width, b = a + m.width;
+  const double xi = (2.0 * T - (a + b)) / (b - a);
+  const double* base = c_rys_tab + m.off + ((size_t)s * N + r) * 2 * RYS_NC;
+  x = chebev<double>(base, xi);
+  w = chebev<double>(base + RYS_NC, xi);
+}
+
+// Where the FP32 launches generate roots and weights in FP64: every
+// quadrature of five or more roots (high angular momentum,
+// l_a + l_b + l_c + l_d >= 8), and T in the last two Chebyshev subintervals
+// below the asymptotic crossover, where the Clenshaw sums lose digits (the
+// reference's own FP64 weights lose three to four there, src/math/rys.rs:
+// 80-89).  Above the crossover the roots and weights are the closed forms
+// c_i / T and w_i T^{-1/2}, exact to FP32 rounding.
+constexpr int ROOTS64_NR = 5;
+template <int N, typename R>
+__device__ __forceinline__ bool roots_in_fp64(R T) {
+  if constexpr (sizeof(R) == 8) {
+    return false;
+  } else {
+    const RysMeta m = c_rys[N];
+    return N >= ROOTS64_NR || (T < R(m.t_hi) && T >= R(m.t_hi - 2.0 * m.width));
+  }
+}
+
 // ----------------------------------------------------------- misc device
 
 __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {

@@ -175,6 +175,10 @@ struct KernelArgs {
   unsigned* store_fault; // MODE_DF3 / MODE_DF2 / MODE_BLOCK: set when an index falls outside `dense`
   int blk_shells[4];     // MODE_BLOCK: requested shells (i, j, k, l)
   int blk_dims[4];       // MODE_BLOCK: their function counts
+  // FP32 launches of the mixed J/K path: a primitive quartet whose magnitude
+  // bound |E_ab E_cd| 2 pi^{5/2} / (p q sqrt(p + q)) is below prim_cut is
+  // skipped (0: every primitive quartet is evaluated)
+  double prim_cut;
 };
 
 }  // namespace igpu

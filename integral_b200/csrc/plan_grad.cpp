@@ -89,8 +89,7 @@ int igpu_grad_device(igpu_plan* P, const igpu_term* coulomb, int ncoul, const ig
     CK(cudaStreamSynchronize(s));
     double dmax = 0.0;
     for (double v : hb) dmax = std::max(dmax, v);
-    fp64_cut = dmax > 0.0 ? P->mixed_cutoff / dmax : std::numeric_limits<double>::infinity();
-    if (fp64_cut <= 0.0) fp64_cut = std::numeric_limits<double>::min();
+    fp64_cut = mixed_split(P->mixed_cutoff, dmax);
   } else {
     CK(cudaStreamSynchronize(s));
   }

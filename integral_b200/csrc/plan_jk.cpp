@@ -46,15 +46,15 @@ int igpu_jk_device(igpu_plan* P, const double* d_dens, int ndens, const uint32_t
   CK(cudaMemcpyAsync(&asym, P->d_flag.p, sizeof(asym), cudaMemcpyDeviceToHost, s));
   CK(cudaMemsetAsync(P->d_counters.p, 0, sizeof(Counters), s));
   // FP64 part: Q_bra*Q_ket*max|D| >= cutoff (the bounds' global max)
-  double fp64_cut = 0.0;
+  double fp64_cut = 0.0, prim_cut = 0.0;
   if (precision == IGPU_PRECISION_MIXED) {
     std::vector<double> hb(nn * ndens);
     CK(cudaMemcpyAsync(hb.data(), P->d_bounds.p, hb.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     double dmax = 0.0;
     for (double v : hb) dmax = std::max(dmax, v);
-    fp64_cut = dmax > 0.0 ? P->mixed_cutoff / dmax : std::numeric_limits<double>::infinity();
-    if (fp64_cut <= 0.0) fp64_cut = std::numeric_limits<double>::min();
+    fp64_cut = mixed_split(P->mixed_cutoff, dmax);
+    if (dmax > 0.0) prim_cut = P->mixed_prim_cut / dmax;
   } else {
     CK(cudaStreamSynchronize(s));
   }
@@ -69,6 +69,7 @@ int igpu_jk_device(igpu_plan* P, const double* d_dens, int ndens, const uint32_t
   A.jk.want_k = want_k ? 1 : 0;
   A.jk.symmetric = asym == 0 ? 1 : 0;
   A.jk.threshold = threshold;
+  A.prim_cut = prim_cut;
   A.bra_bitmap = bra_subset ? P->d_bitmap.p : nullptr;
   const size_t n2 = (size_t)P->nao * P->nao * ndens;
   if (A.jk.symmetric) {

@@ -84,6 +84,19 @@ struct TeamShape {
   static constexpr int TEAM_BYTES = ((TAB_BYTES > STAGE_BYTES ? TAB_BYTES : STAGE_BYTES) + 15) / 16 * 16;
 };
 
+// Magnitude bound of one primitive quartet's contribution, |E_ab E_cd| times
+// the Coulomb prefactor 2 pi^{5/2} / (p q sqrt(p + q)) (every Rys weight sum
+// and Boys value is <= 1); evaluated in FP32 for the primitive screen of the
+// FP32 launches.
+__device__ __forceinline__ float prim_bound(const PrimPairD& b, const PrimPairD& k) {
+  const float p = (float)b.zeta, q = (float)k.zeta;
+  return fabsf((float)b.e * (float)k.e) * (34.98683665f / (p * q * sqrtf(p + q)));
+}
+
+// Largest primitive-quartet count the team screen compacts (16 x 16 primitive
+// pairs); quartets with more run every primitive quartet.
+constexpr int MAX_SURV = 256;
+
 // ------------------------------------------------------------- TEAM == 1
 
 template <int LA, int LB, int LC, int LD, typename R>
@@ -93,13 +106,33 @@ __device__ __forceinline__ void accumulate_thread(const KernelArgs& A, const R* 
   constexpr int NE = S::NE, NF = S::NF, NR = S::NR;
 #pragma unroll
   for (int q = 0; q < S::NG; ++q) G[q] = R(0);
+  const float cut = (sizeof(R) == 4 && A.fp32) ? (float)A.prim_cut : 0.f;
   for (int ip = 0; ip < pb.nprim; ++ip) {
     const PrimPairD bp = A.prims[pb.prim_off + ip];
     for (int kq = 0; kq < pk.nprim; ++kq) {
       const PrimPairD kp = A.prims[pk.prim_off + kq];
+      if constexpr (sizeof(R) == 4)
+        if (cut > 0.f && prim_bound(bp, kp) < cut) continue;
       const QuartetHdr<R> h = quartet_header<R>(bp, kp, A.omega);
       R x[NR], w[NR];
-      rys_roots_s<NR, R>(s_tab, h.T, x, w);
+      if constexpr (sizeof(R) == 4) {
+        // FP32 launch: high l and T just below the asymptotic crossover take
+        // FP64 roots and weights
+        if (roots_in_fp64<NR, R>(h.T)) {
+          const double T64 = quartet_T64(bp, kp, A.omega);
+#pragma unroll
+          for (int r = 0; r < NR; ++r) {
+            double xd, wd;
+            rys_root_fp64<NR>(T64, r, xd, wd);
+            x[r] = R(xd);
+            w[r] = R(wd);
+          }
+        } else {
+          rys_roots_s<NR, R>(s_tab, h.T, x, w);
+        }
+      } else {
+        rys_roots_s<NR, R>(s_tab, h.T, x, w);
+      }
       const R inv_pq = R(1) / h.pq;
       const R qpq = h.q * inv_pq, ppq = h.p * inv_pq;
       const R inv2pq = R(0.5) * inv_pq, inv2p = R(0.5) / h.p, inv2q = R(0.5) / h.q;
@@ -161,7 +194,8 @@ __device__ __forceinline__ void rys_root_one(const R* s_tab, R T, int r, R& x, R
 // [F0, F0 + FCH) of this lane's rows.
 template <int LA, int LB, int LC, int LD, typename R, int F0>
 __device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, const PairD& pb, const PairD& pk,
-                                          R* sm, int lane, unsigned tmask, double* G) {
+                                          R* sm, int lane, unsigned tmask, double* G, const unsigned short* surv,
+                                          int npr) {
   using S = ClassShape<LA, LB, LC, LD>;
   using TS = TeamShape<LA, LB, LC, LD, R>;
   constexpr int NE = S::NE, NF = S::NF, NR = S::NR, T = TS::T;
@@ -186,7 +220,6 @@ __device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, c
   // accumulates its rows over the whole round.
   constexpr int BP = TS::BP, SUB = TS::SUB, PT = TS::PRIM_TAB;
   const int npk = pk.nprim;
-  const int npr = pb.nprim * npk;
   const int myp = lane % BP;
   const int sub = lane / BP;
   for (int base = 0; base < npr; base += BP) {
@@ -195,12 +228,25 @@ __device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, c
     R* mys = sm + myp * PT;
     QuartetHdr<R> h;
     if (active) {
-      const int pidx = base + myp;
+      const int pidx = surv ? (int)surv[base + myp] : base + myp;
       const int ip = pidx / npk, kq = pidx - ip * npk;
-      h = quartet_header<R>(A.prims[pb.prim_off + ip], A.prims[pk.prim_off + kq], A.omega);
+      const PrimPairD& bpp = A.prims[pb.prim_off + ip];
+      const PrimPairD& kpp = A.prims[pk.prim_off + kq];
+      h = quartet_header<R>(bpp, kpp, A.omega);
+      // FP32 launch: high l and T just below the asymptotic crossover take
+      // FP64 roots and weights
+      const bool r64 = roots_in_fp64<NR, R>(h.T);
+      const double T64 = r64 ? quartet_T64(bpp, kpp, A.omega) : 0.0;
       for (int r = sub; r < NR; r += SUB) {
         R xr, wr;
-        rys_root_one<NR, R>(s_tab, h.T, r, xr, wr);
+        if (r64) {
+          double xd, wd;
+          rys_root_fp64<NR>(T64, r, xd, wd);
+          xr = R(xd);
+          wr = R(wd);
+        } else {
+          rys_root_one<NR, R>(s_tab, h.T, r, xr, wr);
+        }
         mys[r] = xr * h.xs;
         mys[NR + r] = wr * h.pref;
       }
@@ -269,13 +315,38 @@ __device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, c
 
 template <int LA, int LB, int LC, int LD, typename R, int C>
 __device__ __forceinline__ void team_chunks(const KernelArgs& A, const R* s_tab, const PairD& pb, const PairD& pk,
-                                            R* sm, int lane, unsigned tmask, double* G) {
+                                            R* sm, int lane, unsigned tmask, double* G, const unsigned short* surv,
+                                            int npr) {
   using TS = TeamShape<LA, LB, LC, LD, R>;
   if constexpr (C < TS::NCHUNK) {
-    team_pass<LA, LB, LC, LD, R, C * TS::FCH>(A, s_tab, pb, pk, sm, lane, tmask, G);
+    team_pass<LA, LB, LC, LD, R, C * TS::FCH>(A, s_tab, pb, pk, sm, lane, tmask, G, surv, npr);
     __syncwarp(tmask);
-    team_chunks<LA, LB, LC, LD, R, C + 1>(A, s_tab, pb, pk, sm, lane, tmask, G);
+    team_chunks<LA, LB, LC, LD, R, C + 1>(A, s_tab, pb, pk, sm, lane, tmask, G, surv, npr);
   }
+}
+
+// Primitive screen of one quartet on a team of T lanes: the indices
+// ip * nprim_ket + kq of the primitive quartets whose bound reaches `cut`,
+// in order, into `list`; returns their count.
+template <int T>
+__device__ __forceinline__ int screen_prims(const KernelArgs& A, const PairD& pb, const PairD& pk, float cut,
+                                            unsigned short* list, int lane, unsigned tmask) {
+  const int npk = pk.nprim, npr = pb.nprim * npk;
+  const int shift = ((threadIdx.x & 31) / T) * T;  // the team's first lane in the warp
+  int n = 0;
+  for (int b0 = 0; b0 < npr; b0 += T) {
+    const int pidx = b0 + lane;
+    bool keep = false;
+    if (pidx < npr) {
+      const int ip = pidx / npk, kq = pidx - ip * npk;
+      keep = prim_bound(A.prims[pb.prim_off + ip], A.prims[pk.prim_off + kq]) >= cut;
+    }
+    const unsigned bal = (__ballot_sync(tmask, keep) & tmask) >> shift;
+    if (keep) list[n + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)pidx;
+    n += __popc(bal);
+  }
+  __syncwarp(tmask);
+  return n;
 }
 
 // ------------------------------------------------------------------ kernel
@@ -285,20 +356,25 @@ __device__ __forceinline__ void team_chunks(const KernelArgs& A, const R* s_tab,
 // allocation, whose unrolled J/K sums take up to 255), thread-per-quartet
 // classes by the size of their register-resident G table (spilling large
 // tables costs more than the occupancy gains).
-template <int LA, int LB, int LC, int LD>
+#ifndef IGPU_FP32_TEAM_MINB
+#define IGPU_FP32_TEAM_MINB 3
+#endif
+template <int LA, int LB, int LC, int LD, typename R>
 __host__ __device__ constexpr int quartet_min_blocks() {
   return team_size<LA, LB, LC, LD>() > 1
-             ? 3
+             ? (sizeof(R) == 4 ? IGPU_FP32_TEAM_MINB : 3)
              : (ClassShape<LA, LB, LC, LD>::NG <= 9 ? 5 : (ClassShape<LA, LB, LC, LD>::NG <= 27 ? 3 : 1));
 }
 
 template <int LA, int LB, int LC, int LD, typename R>
-__global__ void __launch_bounds__(128, quartet_min_blocks<LA, LB, LC, LD>()) quartet_kernel(KernelArgs A) {
+__global__ void __launch_bounds__(128, quartet_min_blocks<LA, LB, LC, LD, R>()) quartet_kernel(KernelArgs A) {
   using S = ClassShape<LA, LB, LC, LD>;
   using TS = TeamShape<LA, LB, LC, LD, R>;
   constexpr int T = TS::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ R s_tab[S::NR * RYS_MAX_SUB * 2 * RYS_NC];
+  constexpr bool SCREEN = sizeof(R) == 4 && T > 1;
+  __shared__ unsigned short s_surv[SCREEN ? (128 / T) * MAX_SURV : 1];
   stage_rys_table<S::NR, R>(s_tab);
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int team = tid / T;
@@ -360,10 +436,23 @@ __global__ void __launch_bounds__(128, quartet_min_blocks<LA, LB, LC, LD>()) qua
 #pragma unroll
         for (int q = 0; q < S::NG; ++q) slot[q] = (double)G[q];
       } else {
-        team_chunks<LA, LB, LC, LD, R, 0>(A, s_tab, pb, pk, sm, lane, tmask, slot);
+        const unsigned short* surv = nullptr;
+        int npr = pb.nprim * pk.nprim;
+        if constexpr (SCREEN) {
+          if (A.fp32 && A.prim_cut > 0.0 && npr <= MAX_SURV) {
+            unsigned short* list = s_surv + (threadIdx.x / T) * MAX_SURV;
+            npr = screen_prims<T>(A, pb, pk, (float)A.prim_cut, list, lane, tmask);
+            surv = list;
+            if (npr == 0) continue;  // the whole quartet is below the screen
+          }
+        }
+        team_chunks<LA, LB, LC, LD, R, 0>(A, s_tab, pb, pk, sm, lane, tmask, slot, surv, npr);
       }
       __syncwarp(tmask);
-      if constexpr (T > 1) {
+      // the compile-time shaped J/K sums unroll over the whole Cartesian
+      // block; blocks beyond (ff|ff) (g shells) take the runtime post phase
+      constexpr bool CT_POST = ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD) <= 10000;
+      if constexpr (T > 1 && CT_POST) {
         if (use_acc && A.kinds == 0) {
           post_quartet_jk_cart<LA, LB, LC, LD, T>(A, pb, pk, sc, slot, lane, tmask, pbi, stage);
           continue;
