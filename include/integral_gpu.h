@@ -56,9 +56,11 @@ extern "C" {
 #define IGPU_ENGINE_RYS 2
 
 /* Arithmetic of the quartet kernels.  FP64: every quartet in double.
- * MIXED: quartets whose Schwarz estimate Q_ij*Q_kl*max|D| is below the
- * plan's cutoff run their Rys roots, recurrences and contraction in FP32,
- * the rest in FP64; all J/K/gradient accumulation is FP64. */
+ * MIXED: quartets whose Schwarz estimate Q_ij*Q_kl*M is below the plan's
+ * cutoff run their Rys roots, recurrences and contraction in FP32, the rest
+ * in FP64; M is max|D| (or the term matrices' maximum) rounded up to a power
+ * of two, so densities whose maxima share a binade share one task list.  All
+ * J/K/gradient accumulation is FP64. */
 #define IGPU_PRECISION_FP64 0
 #define IGPU_PRECISION_MIXED 1
 
@@ -145,6 +147,13 @@ int igpu_schwarz(const igpu_plan* plan, double* q);
 int igpu_schwarz_bounds(const igpu_shell* shells, size_t nsh, double* q, size_t* n_rys);
 /* Plan cutoff for IGPU_PRECISION_MIXED (default 1e-4). */
 int igpu_set_mixed_cutoff(igpu_plan* plan, double cutoff);
+/* Primitive screen of the FP32 quartets of IGPU_PRECISION_MIXED J/K (no
+ * counterpart in the reference, which evaluates every primitive quartet that
+ * survives its 1e-32 pair screen): inside an FP32 quartet, a primitive
+ * quartet whose magnitude bound |E_ab E_cd| 2 pi^{5/2} / (p q sqrt(p + q))
+ * times max|D| is below eps is skipped (default 1e-15).  0 evaluates every
+ * primitive quartet; the FP64 path never skips one. */
+int igpu_set_mixed_prim_cutoff(igpu_plan* plan, double eps);
 /* EriKernel (src/integrals.rs:304-321) of every later call on the plan:
  * omega = 0 is Coulomb 1/r (the default); omega > 0 finite is the long-range
  * erf(omega r)/r (Basis::eri_kernel, EriBuilder::kernel, the gradient's
@@ -255,6 +264,35 @@ int igpu_grad(igpu_plan* plan, const igpu_term* coulomb, int ncoul, const igpu_t
 int igpu_grad_device(igpu_plan* plan, const igpu_term* d_coulomb, int ncoul,
                      const igpu_term* d_exchange, int nexch, const uint32_t* bra_subset,
                      size_t nsub, double threshold, int precision, double* d_out, void* stream);
+
+/* Molecule batches (no counterpart in the reference, whose callers loop
+ * over one DirectContractor / DirectGradContractor per molecule,
+ * src/direct.rs:19-21, src/direct_grad.rs:140-142).  A batch holds many
+ * independent molecules of uneven size: molecule m has mol_nsh[m] shells,
+ * consecutive in `shells`.  Each step runs, for every molecule, one direct
+ * J/K build with its own density and, optionally, the density-direct
+ * gradient of E = coul_factor * tr(D J[D])-type and exch_factor *
+ * tr(D K[D])-type terms (GradDensityTerm (coul_factor, D, D) and
+ * (exch_factor, D, D)), with exactly the screening, integrals and
+ * contractions of a plan of that molecule alone.  Every angular class of
+ * every molecule runs in one persistent launch per class; the first step
+ * with a given (threshold, precision split, want_k, want_grad, factors,
+ * density symmetry) captures the whole sequence into a CUDA graph, later
+ * steps replay it. */
+typedef struct igpu_batch igpu_batch;
+int igpu_batch_create(const igpu_shell* shells, const size_t* mol_nsh, size_t nmol, igpu_batch** out);
+int igpu_batch_destroy(igpu_batch* batch);
+/* nao, natom (bitwise-equal centres inside the molecule) and nsh of molecule `mol`. */
+int igpu_batch_query(const igpu_batch* batch, size_t mol, size_t* nao, size_t* natom, size_t* nsh);
+/* One step over host buffers.  dens, J and K hold the molecules' nao_m x
+ * nao_m matrices back to back (row-major); grad holds natom_m x 3 per
+ * molecule back to back (dE/dR).  J, K and grad accumulate (+=).  stats
+ * (may be NULL) receives the step's counters: kernel_ms is the device time
+ * of the graph launch, launches the kernels it ran. */
+int igpu_batch_jk_grad(igpu_batch* batch, const double* dens, double threshold, int precision, int want_k,
+                       int want_grad, double coul_factor, double exch_factor, double* J, double* K, double* grad,
+                       igpu_stats* stats);
+int igpu_batch_set_mixed_cutoff(igpu_batch* batch, double cutoff);
 
 /* Counters of the last J/K or gradient call on the plan. */
 int igpu_last_stats(const igpu_plan* plan, igpu_stats* stats);

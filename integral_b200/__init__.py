@@ -808,6 +808,12 @@ class DirectContractor:
         (default 1e-4) run in FP32 (igpu_set_mixed_cutoff)."""
         _lib.check(_lib.lib().igpu_set_mixed_cutoff(self._plan.h, float(cutoff)))
 
+    def set_mixed_prim_cutoff(self, eps: float):
+        """MIXED precision: inside the FP32 quartets, skip primitive quartets
+        whose magnitude bound times max|D| is below `eps`
+        (igpu_set_mixed_prim_cutoff; 0 evaluates all of them)."""
+        _lib.check(_lib.lib().igpu_set_mixed_prim_cutoff(self._plan.h, float(eps)))
+
     def jk_device_static(self, d_dens, ndens, d_J, d_K, threshold, want_exchange=True, stream=None):
         """FP64 J/K on device pointers that allocates no device memory
         (igpu_jk_device_static), for callers whose device memory belongs to
@@ -945,3 +951,89 @@ class DirectGradContractor:
 
 def abi_version() -> int:
     return int(_lib.lib().igpu_abi_version())
+
+
+class MoleculeBatch:
+    """Many independent molecules of uneven size in one batch
+    (igpu_batch_*).  No reference counterpart: the reference's callers loop
+    over one DirectContractor / DirectGradContractor per molecule
+    (src/direct.rs:19-21, src/direct_grad.rs:140-142).  One step runs, for
+    every molecule, the J/K build of its density and (optionally) the
+    density-direct gradient of the Coulomb term (coulomb_factor, D, D) and
+    the exchange term (exchange_factor, D, D), each molecule screened and
+    evaluated exactly as its own plan would; every angular class of every
+    molecule runs in one persistent launch, and the step is a CUDA graph
+    captured on first use and replayed afterwards."""
+
+    def __init__(self, molecules: Sequence[Sequence[Shell]]):
+        L = _lib.lib()
+        mols = [[s if isinstance(s, Shell) else Shell.from_dict(s) for s in m] for m in molecules]
+        flat = [s for m in mols for s in m]
+        self._keep = []
+        arr = _Plan._shell_array(flat, self._keep)
+        counts = np.array([len(m) for m in mols], dtype=np.uintp)
+        self._keep.append(counts)
+        h = ctypes.c_void_p()
+        _lib.check(L.igpu_batch_create(arr, counts.ctypes.data_as(_lib.c_size_p), len(mols), ctypes.byref(h)))
+        self.h = h
+        self._nao, self._natom = [], []
+        for m in range(len(mols)):
+            nao, natom, nsh = (ctypes.c_size_t() for _ in range(3))
+            _lib.check(L.igpu_batch_query(h, m, ctypes.byref(nao), ctypes.byref(natom), ctypes.byref(nsh)))
+            self._nao.append(nao.value)
+            self._natom.append(natom.value)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                _lib.lib().igpu_batch_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def __len__(self) -> int:
+        return len(self._nao)
+
+    def nao(self, m: int) -> int:
+        return self._nao[m]
+
+    def natom(self, m: int) -> int:
+        return self._natom[m]
+
+    def set_mixed_cutoff(self, cutoff: float):
+        _lib.check(_lib.lib().igpu_batch_set_mixed_cutoff(self.h, float(cutoff)))
+
+    def jk_grad(self, densities, threshold: float, precision: int = 0, want_exchange: bool = True,
+                gradient: bool = True, coulomb_factor: float = 0.5, exchange_factor: float = -0.25):
+        """densities: one nao_m x nao_m matrix per molecule.  Returns lists of
+        J, K (None without exchange) and gradients (natom_m x 3, None without
+        gradient) per molecule."""
+        if len(densities) != len(self._nao):
+            raise IntegralError(-7, "length mismatch", "one density per molecule")
+        for D, n in zip(densities, self._nao):
+            if np.shape(D) != (n, n):
+                raise IntegralError(-7, "length mismatch", "density of shape (%d, %d) expected" % (n, n))
+        dens = np.ascontiguousarray(np.concatenate([np.asarray(D, dtype=np.float64).reshape(-1)
+                                                    for D in densities]))
+        J = np.zeros_like(dens)
+        K = np.zeros_like(dens) if want_exchange else None
+        G = np.zeros(3 * sum(self._natom)) if gradient else None
+        st = IgpuStats()
+        _lib.check(_lib.lib().igpu_batch_jk_grad(
+            self.h, dens.ctypes.data_as(c_double_p), float(threshold), int(precision), int(bool(want_exchange)),
+            int(bool(gradient)), float(coulomb_factor), float(exchange_factor), J.ctypes.data_as(c_double_p),
+            K.ctypes.data_as(c_double_p) if K is not None else None,
+            G.ctypes.data_as(c_double_p) if G is not None else None, ctypes.byref(st)))
+        self._stats = {f: getattr(st, f) for f, _ in IgpuStats._fields_}
+        out_j, out_k, out_g = [], [], []
+        o = og = 0
+        for n, na in zip(self._nao, self._natom):
+            out_j.append(J[o:o + n * n].reshape(n, n))
+            out_k.append(K[o:o + n * n].reshape(n, n) if K is not None else None)
+            out_g.append(G[og:og + 3 * na].reshape(na, 3) if G is not None else None)
+            o += n * n
+            og += 3 * na
+        return out_j, out_k, out_g
+
+    def last_stats(self) -> dict:
+        return dict(getattr(self, "_stats", {}))

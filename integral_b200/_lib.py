@@ -69,6 +69,7 @@ def lib():
     L.igpu_schwarz.argtypes = [vp, c_double_p]
     L.igpu_schwarz_bounds.argtypes = [ctypes.POINTER(IgpuShell), ctypes.c_size_t, c_double_p, c_size_p]
     L.igpu_set_mixed_cutoff.argtypes = [vp, ctypes.c_double]
+    L.igpu_set_mixed_prim_cutoff.argtypes = [vp, ctypes.c_double]
     L.igpu_set_erf_omega.argtypes = [vp, ctypes.c_double]
     L.igpu_eri_dense.argtypes = [vp, c_double_p]
     L.igpu_eri_builder_fill.argtypes = [vp, c_u32_p, ctypes.c_size_t, c_double_p]
@@ -96,18 +97,26 @@ def lib():
     L.igpu_autotune_jk.argtypes = [vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, vp]
     L.igpu_autotune_grad.argtypes = [vp, ctypes.POINTER(IgpuTerm), ctypes.c_int, ctypes.POINTER(IgpuTerm),
                                      ctypes.c_int, ctypes.c_double, ctypes.c_int]
+    L.igpu_batch_create.argtypes = [ctypes.POINTER(IgpuShell), c_size_p, ctypes.c_size_t, ctypes.POINTER(vp)]
+    L.igpu_batch_destroy.argtypes = [vp]
+    L.igpu_batch_query.argtypes = [vp, ctypes.c_size_t, c_size_p, c_size_p, c_size_p]
+    L.igpu_batch_jk_grad.argtypes = [vp, c_double_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_double, ctypes.c_double, c_double_p, c_double_p, c_double_p,
+                                     ctypes.POINTER(IgpuStats)]
+    L.igpu_batch_set_mixed_cutoff.argtypes = [vp, ctypes.c_double]
     _lib = L
     return L
 
 
 EXPORTED = [
     "igpu_abi_version", "igpu_last_error_string", "igpu_plan_create", "igpu_plan_destroy", "igpu_plan_query",
-    "igpu_bra_pairs", "igpu_atoms", "igpu_schwarz", "igpu_schwarz_bounds", "igpu_set_mixed_cutoff", "igpu_set_erf_omega",
+    "igpu_bra_pairs", "igpu_atoms", "igpu_schwarz", "igpu_schwarz_bounds", "igpu_set_mixed_cutoff", "igpu_set_mixed_prim_cutoff", "igpu_set_erf_omega",
     "igpu_eri_dense",
     "igpu_eri_builder_fill", "igpu_eri_screened", "igpu_eri_block", "igpu_eri_packed", "igpu_plan_attach_aux", "igpu_aux_query", "igpu_schwarz_aux",
     "igpu_eri_2c", "igpu_eri_3c", "igpu_density_shell_bounds", "igpu_jk", "igpu_jk_device", "igpu_jk_device_static",
     "igpu_grad",
     "igpu_grad_device", "igpu_last_stats", "igpu_last_profile", "igpu_autotune_jk", "igpu_autotune_grad",
+    "igpu_batch_create", "igpu_batch_destroy", "igpu_batch_query", "igpu_batch_jk_grad", "igpu_batch_set_mixed_cutoff",
 ]
 
 

@@ -241,4 +241,57 @@ cudaError_t launch_asym_count(const double* D, int nmat, int nao, unsigned long 
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------ molecule batches
+//
+// A batch stores molecule m's nao x nao matrices with row stride P (the
+// largest molecule's AO count) at m*P*(P+1), and its nsh x nsh shell-block
+// bounds with row stride S (the largest shell count) at m*S*(S+1): the
+// addresses that global indices m*P + local (AOs) and m*S + local (shells)
+// give in a row-major P- or S-stride matrix.
+
+// Shell-block maxima of every molecule's density (src/direct.rs:103-125;
+// with `symmetrise` the max over (i,j) and (j,i), src/direct_grad.rs:292-312).
+__global__ void batch_block_max_kernel(const double* __restrict__ D, const DevShell* __restrict__ sh, int nmol,
+                                       int S, int P, int symmetrise, double* __restrict__ out) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t per = (size_t)S * S;
+  if (t >= per * nmol) return;
+  const int m = (int)(t / per);
+  const int r = (int)(t % per);
+  const int i = m * S + r / S, j = m * S + r % S;
+  const DevShell si = sh[i], sj = sh[j];
+  double mx = 0.0;
+  for (int a = 0; a < si.nfunc; ++a)
+    for (int b = 0; b < sj.nfunc; ++b) mx = fmax(mx, fabs(D[(size_t)(si.off + a) * P + sj.off + b]));
+  if (symmetrise)
+    for (int a = 0; a < sj.nfunc; ++a)
+      for (int b = 0; b < si.nfunc; ++b) mx = fmax(mx, fabs(D[(size_t)(sj.off + a) * P + si.off + b]));
+  out[(size_t)i * S + j] = mx;  // = m*S*(S+1) + i_local*S + j_local
+}
+
+cudaError_t launch_batch_block_max(const double* D, const DevShell* sh, int nmol, int S, int P, int symmetrise,
+                                   double* out, cudaStream_t s) {
+  const size_t n = (size_t)S * S * nmol;
+  if (n == 0) return cudaSuccess;
+  batch_block_max_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(D, sh, nmol, S, P, symmetrise, out);
+  return cudaGetLastError();
+}
+
+// out_m += (H_m + H_m^T) / 2 for every molecule block.
+__global__ void batch_symmetrize_add_kernel(const double* __restrict__ H, double* __restrict__ out, int nmol, int P) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t per = (size_t)P * P;
+  if (t >= per * nmol) return;
+  const size_t m = t / per, r = (t % per) / P, c = t % P;
+  const size_t base = m * (size_t)P * (P + 1);
+  out[base + r * P + c] += 0.5 * (H[base + r * P + c] + H[base + c * P + r]);
+}
+
+cudaError_t launch_batch_symmetrize_add(const double* H, double* out, int nmol, int P, cudaStream_t s) {
+  const size_t n = (size_t)P * P * nmol;
+  if (n == 0) return cudaSuccess;
+  batch_symmetrize_add_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(H, out, nmol, P);
+  return cudaGetLastError();
+}
+
 }  // namespace igpu

@@ -41,5 +41,10 @@ cudaError_t launch_shell_block_max(const double* D, int nmat, const DevShell* sh
                                    int symmetrise, double* out, cudaStream_t s);
 cudaError_t launch_symmetrize_add(const double* H, double* out, int nmat, int nao, cudaStream_t s);
 cudaError_t launch_asym_count(const double* D, int nmat, int nao, unsigned long long* flag, cudaStream_t s);
+// Molecule batches (plan_batch.cpp): matrices of molecule m at m*P*(P+1),
+// row stride P; shell blocks at m*S*(S+1), row stride S.
+cudaError_t launch_batch_block_max(const double* D, const DevShell* sh, int nmol, int S, int P, int symmetrise,
+                                   double* out, cudaStream_t s);
+cudaError_t launch_batch_symmetrize_add(const double* H, double* out, int nmol, int P, cudaStream_t s);
 
 }  // namespace igpu

@@ -152,6 +152,20 @@ double model_flops_grad_quartet(int la, int lb, int lc, int ld, bool sph, int nt
   return f;
 }
 
+// Q_bra * Q_ket at or above which a quartet of the MIXED path runs in FP64:
+// the plan's cutoff over max|D| rounded up to a power of two.  Rounding up
+// keeps every quartet with Q_bra * Q_ket * max|D| >= cutoff in FP64, and
+// the densities of successive SCF iterations, whose maxima rarely leave
+// their binade, then share one cached task list.
+double mixed_split(double cutoff, double dmax) {
+  if (!(dmax > 0.0)) return std::numeric_limits<double>::infinity();
+  int e = 0;
+  const double m = std::frexp(dmax, &e);
+  const double up = m == 0.5 ? dmax : std::ldexp(1.0, e);
+  const double cut = cutoff / up;
+  return cut > 0.0 ? cut : std::numeric_limits<double>::min();
+}
+
 // Key of a launch class in the tuned-chunk table; gradient classes have
 // their own keys.
 int tune_key(int pcb, int pck, bool fp32, bool grad) {
@@ -161,7 +175,7 @@ int tune_key(int pcb, int pck, bool fp32, bool grad) {
 // Chunk tuning: note every launch time of the last call made at chunk
 // multiplier m, then keep per class the multiplier of the shortest time.
 void tune_record(igpu_plan* P, int m, bool grad, std::map<int, std::map<int, float>>& best) {
-  for (const igpu_launch_record& r : P->profile) {
+  for (const igpu_launch_record& r : P->log.profile) {
     auto& slot = best[tune_key(pair_class(r.la, r.lb), pair_class(r.lc, r.ld), r.fp32 != 0, grad)];
     auto it = slot.find(m);
     if (it == slot.end() || r.ms < it->second) slot[m] = r.ms;
@@ -203,17 +217,18 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
   }
   CK(P->d_scratch.ensure(need));
   const size_t nl = ts.launches.size();
-  CK(P->d_launch_counters.ensure(nl));
-  CK(cudaMemsetAsync(P->d_launch_counters.p, 0, nl * sizeof(Counters), s));
-  CK(P->d_work.ensure(nl));
-  CK(cudaMemsetAsync(P->d_work.p, 0, nl * sizeof(unsigned long long), s));
-  while (P->events.size() < 2 * nl) {
+  LaunchLog& lg = *P->cur_log;
+  CK(lg.counters.ensure(nl));
+  CK(cudaMemsetAsync(lg.counters.p, 0, nl * sizeof(Counters), s));
+  CK(lg.work.ensure(nl));
+  CK(cudaMemsetAsync(lg.work.p, 0, nl * sizeof(unsigned long long), s));
+  while (lg.events.size() < 2 * nl) {
     cudaEvent_t ev;
     CK(cudaEventCreate(&ev));
-    P->events.push_back(ev);
+    lg.events.push_back(ev);
   }
-  P->profile.clear();
-  P->profile_launch.clear();
+  lg.profile.clear();
+  lg.profile_launch.clear();
   for (size_t li = 0; li < nl; ++li) {
     Launch* L = ts.launches[li].get();
     if (L->total == 0) continue;
@@ -222,7 +237,7 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     A.scratch = P->d_scratch.p;
     A.slot_doubles = slot_with_acc(e, L->pcb, A);
     A.acc_offset = e->slot;
-    A.work_counter = P->d_work.p + li;
+    A.work_counter = lg.work.p + li;
     int mult = 16;
     if (P->tune_mult) {
       mult = P->tune_mult;
@@ -231,7 +246,7 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
       if (t != P->tuned_mult.end()) mult = t->second;
     }
     A.chunk = (unsigned long long)(32 / e->team) * mult;
-    if (A.counters) A.counters = P->d_launch_counters.p + li;
+    if (A.counters) A.counters = lg.counters.p + li;
     A.task.bra_pair = L->bra_pair.p;
     A.task.ket_pairs = L->ket_list;
     A.task.prefix = L->prefix.p;
@@ -240,9 +255,9 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     A.task.total = L->total;
     A.fp32 = L->fp32 ? 1 : 0;
     A.builder_swap = L->builder_swap;
-    CK(cudaEventRecord(P->events[2 * li], s));
+    CK(cudaEventRecord(lg.events[2 * li], s));
     CK(launch_quartets(e, L->fp32, (int)grid, A, s));
-    CK(cudaEventRecord(P->events[2 * li + 1], s));
+    CK(cudaEventRecord(lg.events[2 * li + 1], s));
     ++launches;
     igpu_launch_record r{};
     r.la = pc_la_host(L->pcb);
@@ -254,23 +269,24 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     r.grid = (uint32_t)grid;
     r.tasks = L->total;
     r.chunk = (uint32_t)A.chunk;
-    P->profile.push_back(r);
-    P->profile_launch.push_back(li);
+    lg.profile.push_back(r);
+    lg.profile_launch.push_back(li);
   }
   return IGPU_OK;
 }
 
 // After the stream is synchronised: per-launch times, counters, model flops.
 int collect_profile(igpu_plan* P, int ndens, bool jk, int grad_terms_c, int grad_terms_x) {
-  const size_t nl = P->profile.empty() ? 0 : P->profile_launch.back() + 1;
+  LaunchLog& lg = *P->cur_log;
+  const size_t nl = lg.profile.empty() ? 0 : lg.profile_launch.back() + 1;
   std::vector<Counters> c(nl);
-  if (nl) CK(cudaMemcpy(c.data(), P->d_launch_counters.p, nl * sizeof(Counters), cudaMemcpyDeviceToHost));
+  if (nl) CK(cudaMemcpy(c.data(), lg.counters.p, nl * sizeof(Counters), cudaMemcpyDeviceToHost));
   P->last = igpu_stats{};
-  for (size_t k = 0; k < P->profile.size(); ++k) {
-    igpu_launch_record& r = P->profile[k];
-    const size_t li = P->profile_launch[k];
+  for (size_t k = 0; k < lg.profile.size(); ++k) {
+    igpu_launch_record& r = lg.profile[k];
+    const size_t li = lg.profile_launch[k];
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, P->events[2 * li], P->events[2 * li + 1]);
+    cudaEventElapsedTime(&ms, lg.events[2 * li], lg.events[2 * li + 1]);
     r.ms = ms;
     r.quartets = c[li].quartets;
     r.prim_quartets = c[li].prim_quartets;
@@ -288,7 +304,7 @@ int collect_profile(igpu_plan* P, int ndens, bool jk, int grad_terms_c, int grad
     P->last.model_flops += r.model_flops;
     P->last.kernel_ms += ms;
   }
-  P->last.launches = (uint32_t)P->profile.size();
+  P->last.launches = (uint32_t)lg.profile.size();
   return IGPU_OK;
 }
 
@@ -348,8 +364,15 @@ int build_jk_tasks(igpu_plan* P, double tau, double fp64_cut, TaskSet& ts) {
       std::vector<int> bras, n64, n32, st64, st32;
       for (size_t bp = 0; bp < B.size(); ++bp) {
         const double qb = P->pairs[B[bp]].q;
-        for (const auto& grp : groups) {
-          const size_t gs = grp.first, ge = grp.second;
+        // a batch pairs a bra with the kets of its own molecule only
+        size_t g0 = 0, g1 = groups.size();
+        if (P->batch) {
+          const auto& r = P->class_mol_groups[cb][P->shells[P->pairs[B[bp]].i].pad];
+          g0 = (size_t)r.first;
+          g1 = (size_t)r.second;
+        }
+        for (size_t gi = g0; gi < g1; ++gi) {
+          const size_t gs = groups[gi].first, ge = groups[gi].second;
           if (ca == cb && gs > bp) break;  // kets at class positions <= bp only
           size_t lo = gs, hi = ge;  // first ket with qb*qk < tau
           while (lo < hi) {
@@ -467,9 +490,10 @@ int run_schwarz(igpu_plan* P) {
   std::vector<double> q(P->npairs);
   CK(cudaMemcpyAsync(q.data(), P->d_schwarz_pair.p, q.size() * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
   CK(cudaStreamSynchronize(P->stream));
-  P->schwarz.assign((size_t)P->nsh * P->nsh, 0.0);
+  if (!P->batch) P->schwarz.assign((size_t)P->nsh * P->nsh, 0.0);
   for (int p = 0; p < P->npairs; ++p) {
     P->pairs[p].q = q[p];
+    if (P->batch) continue;  // a batch keeps its bounds per pair only
     const int i = P->pairs[p].i, j = P->pairs[p].j;
     P->schwarz[(size_t)i * P->nsh + j] = q[p];
     P->schwarz[(size_t)j * P->nsh + i] = q[p];
@@ -492,6 +516,7 @@ void exact_schwarz(igpu_plan* P) {
     if (!done[p]) continue;
     ++P->schwarz_exact_pairs;
     P->pairs[p].q = q[p];
+    if (P->batch) continue;
     const int i = P->pairs[p].i, j = P->pairs[p].j;
     P->schwarz[(size_t)i * P->nsh + j] = q[p];
     P->schwarz[(size_t)j * P->nsh + i] = q[p];
@@ -707,7 +732,6 @@ int igpu_plan_destroy(igpu_plan* plan) {
   cudaStreamSynchronize(plan->stream);
   if (plan->ev0) cudaEventDestroy(plan->ev0);
   if (plan->ev1) cudaEventDestroy(plan->ev1);
-  for (cudaEvent_t ev : plan->events) cudaEventDestroy(ev);
   cudaStream_t s = plan->stream;
   delete plan;
   if (s) cudaStreamDestroy(s);
@@ -813,6 +837,12 @@ int igpu_set_mixed_cutoff(igpu_plan* P, double cutoff) {
   return IGPU_OK;
 }
 
+int igpu_set_mixed_prim_cutoff(igpu_plan* P, double eps) {
+  if (!P || !(eps >= 0.0) || std::isinf(eps)) return fail(IGPU_ERR_INVALID_ARGUMENT, "invalid primitive cutoff");
+  P->mixed_prim_cut = eps;
+  return IGPU_OK;
+}
+
 int igpu_last_stats(const igpu_plan* P, igpu_stats* st) {
   if (!P || !st) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
   *st = P->last;
@@ -821,8 +851,8 @@ int igpu_last_stats(const igpu_plan* P, igpu_stats* st) {
 
 int igpu_last_profile(const igpu_plan* P, igpu_launch_record* out, size_t cap, size_t* n) {
   if (!P || !n) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
-  *n = P->profile.size();
-  for (size_t k = 0; k < P->profile.size() && k < cap && out; ++k) out[k] = P->profile[k];
+  *n = P->log.profile.size();
+  for (size_t k = 0; k < P->log.profile.size() && k < cap && out; ++k) out[k] = P->log.profile[k];
   return IGPU_OK;
 }
 

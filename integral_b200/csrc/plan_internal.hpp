@@ -89,6 +89,19 @@ struct TaskSet {
   std::vector<std::unique_ptr<Launch>> launches;
 };
 
+// Per-launch counters, work counters, events and records of one run of a
+// task set (run_tasks / collect_profile).
+struct LaunchLog {
+  DevBuf<Counters> counters;
+  DevBuf<unsigned long long> work;
+  std::vector<cudaEvent_t> events;
+  std::vector<igpu_launch_record> profile;
+  std::vector<size_t> profile_launch;
+  ~LaunchLog() {
+    for (cudaEvent_t ev : events) cudaEventDestroy(ev);
+  }
+};
+
 // Mixed-precision J/K task lists kept per plan (see igpu_plan::mixed_keys).
 constexpr size_t kMixedTaskSets = 4;
 
@@ -104,6 +117,15 @@ struct igpu_plan {
   int device = 0;
   int engine = 0;
   int nsh = 0, nao = 0, natom = 0, npairs = 0;
+  // molecule batch (igpu_batch_*): shells of molecule m at global indices
+  // m*nsh + local and AOs at m*nao + local, with nsh and nao the per-molecule
+  // maxima, so that every row-major index the kernels form from them lands
+  // in molecule m's own block at m*nao*(nao+1) (m*nsh*(nsh+1) for shell
+  // blocks); pairs and quartets never cross molecules
+  bool batch = false;
+  // per class, per molecule: its run [first, end) of class_groups[class]
+  std::vector<std::vector<std::pair<int, int>>> class_mol_groups;
+
   bool spherical_any = false;
   std::vector<DevShell> shells;
   std::vector<std::array<double, 3>> atoms;
@@ -133,7 +155,6 @@ struct igpu_plan {
   DevBuf<double> d_schwarz_pair;
   // per-call device buffers
   DevBuf<double> d_D, d_J, d_K, d_bounds, d_dense, d_Jh, d_Kh;
-  DevBuf<unsigned long long> d_work;
   DevBuf<unsigned long long> d_flag;
   DevBuf<unsigned> d_bitmap;
   std::map<std::pair<double, double>, std::unique_ptr<TaskSet>> jk_tasks;  // (threshold, fp64 cutoff)
@@ -147,13 +168,16 @@ struct igpu_plan {
   int tune_mult = 0;
   std::unique_ptr<TaskSet> dense_tasks;
   double mixed_cutoff = 1e-4;
+  // primitive screen of the FP32 launches of the mixed path: bound * max|D|
+  // below this skips a primitive quartet (0: none)
+  double mixed_prim_cut = 1e-15;
   double erf_omega = 0.0;  // 0: Coulomb; > 0: erf(omega r)/r for every later call
   bool all_spherical = false;
   igpu_stats last{};
-  DevBuf<Counters> d_launch_counters;
-  std::vector<cudaEvent_t> events;
-  std::vector<igpu_launch_record> profile;
-  std::vector<size_t> profile_launch;
+  // the launch log of the last J/K or gradient call; a molecule batch logs
+  // its gradient phase in log2 (cur_log selects the one run_tasks fills)
+  LaunchLog log, log2;
+  LaunchLog* cur_log = &log;
   // gradient: term matrices, their block maxima and the device term tables
   DevBuf<double> d_gmat, d_gmax, d_gfac, d_gout;
   DevBuf<const double*> d_gptr;
@@ -181,6 +205,7 @@ double model_flops_prim(int la, int lb, int lc, int ld);
 double model_flops_quartet(int la, int lb, int lc, int ld, bool sph, int ndens, bool jk);
 double model_flops_grad_prim(int la, int lb, int lc, int ld);
 double model_flops_grad_quartet(int la, int lb, int lc, int ld, bool sph, int nterm_c, int nterm_x);
+double mixed_split(double cutoff, double dmax);
 int tune_key(int pcb, int pck, bool fp32, bool grad);
 void tune_record(igpu_plan* P, int m, bool grad, std::map<int, std::map<int, float>>& best);
 void tune_keep(igpu_plan* P, const std::map<int, std::map<int, float>>& best);
