@@ -64,12 +64,13 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-sample-bras", type=int, default=24)
-    p.add_argument("--workload", default="jk", choices=["jk", "grad", "dense", "jk-sph"],
+    p.add_argument("--workload", default="jk", choices=["jk", "grad", "dense", "jk-sph", "batch"],
                    help="jk: the headline J/K build (default); grad: the density-direct ERI gradient of the "
                         "100-atom / nao 1400 system on an interleaved 1/--grad-stride share of the bra pairs; "
                         "dense: the dense nao^4 tensor of the 6-atom / nao 54 system; jk-sph: J/K of the "
                         "200-atom / nao 5200 spherical system on an interleaved 1/--sph-stride share of the "
-                        "bra pairs")
+                        "bra pairs; batch: 256 molecules (s,s,p,p,d,f,g spherical) in one graph-captured "
+                        "step per precision")
     p.add_argument("--sph-stride", type=int, default=512)
     # a stride > 1 still decodes every task (the subset is a filter), so its
     # quartets/s understates the full build's
@@ -110,9 +111,13 @@ def grad_bench(args):
         return out, st, wall
 
     res = {}
+    clocks, prof32, launches = None, None, 0
     for prec in (1, 0):
         for _ in range(args.warmup):
             run(prec)
+        clk = ClockSampler(0) if prec == 1 else None
+        if clk:
+            clk.start()
         ms, q, flops, wall = 0.0, 0, 0.0, 0.0
         for _ in range(args.steps):
             out, st, w = run(prec)
@@ -120,9 +125,27 @@ def grad_bench(args):
             q += st["quartets"]
             flops += st["model_flops"]
             wall += w
+            if prec == 1:
+                launches += st["launches"]
+        if clk:
+            clocks = clk.stop()
+            prof32 = gc._plan.profile()
         res[prec] = (out, ms, q, flops, wall)
     g32, ms32, q32, f32, w32 = res[1]
     g64, ms64, q64, f64, w64 = res[0]
+    top = max(prof32, key=lambda r: r["ms"])
+    pk = measured_gemm_tflops(torch, torch.float32 if top["fp32"] else torch.float64)
+    achieved = top["model_flops"] / (top["ms"] * 1e-3) / 1e12
+    # CPU baseline: the C++ restatement of the reference's gradient path on
+    # every host thread over a seeded sample of canonical bra pairs
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_py as O
+    ob = O.OracleBasis(s["shells"])
+    nthreads = os.cpu_count() or 1
+    sample = np.random.default_rng(11).choice(len(gc.bra_pairs()), 2 * nthreads, replace=False)
+    t0 = time.perf_counter()
+    _, cpu_q, _ = ob.direct_grad(s["coulomb"], s["exchange"], s["threshold"], bras=sample, nthreads=nthreads)
+    cpu_s = time.perf_counter() - t0
     line = {
         "metric": "density-direct ERI gradient quartets/s (FP32-mixed) on B200", "unit": "quartets/s",
         "value": q32 / (ms32 * 1e-3), "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -136,6 +159,21 @@ def grad_bench(args):
         "model_tflops": f32 / (ms32 * 1e-3) / 1e12,
         "max_abs_mixed_minus_fp64": float(np.abs(g32 - g64).max()),
         "max_abs_gradient": float(np.abs(g64).max()),
+        "roofline": {"bound": "fp32" if top["fp32"] else "fp64",
+                     "kernel": "grad_kernel(%d%d|%d%d) %s" % (top["la"], top["lb"], top["lc"], top["ld"],
+                                                              "fp32" if top["fp32"] else "fp64"),
+                     "achieved": achieved, "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk,
+                     "peak_source": "cuBLAS %s GEMM measured in this run (no FP64/FP32 CUDA-core peak in "
+                                    "MEASURED_PEAKS.json)" % ("SGEMM, TF32 off" if top["fp32"] else "DGEMM"),
+                     "flops_model": "fixed Rys flop model: six shifted value classes per surviving primitive "
+                                    "quartet plus the weight-block dots",
+                     "traffic": None},
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "cpu_baseline": {"value": cpu_q / cpu_s, "unit": "quartets/s", "cores": nthreads, "kind": "port",
+                         "sample": "%d seeded canonical bra pairs (%d screened quartets, %.1f s), all threads; C++ "
+                                   "restatement of the reference CPU gradient path (its generic OS/HGP and Rys "
+                                   "engines, not the reference's specialised kernels)" % (len(sample), cpu_q, cpu_s)},
         "e2e": {"value": q32 / w32, "unit": "quartets/s",
                 # the distinct term matrices go up once per call, the natom x 3 gradient comes back
                 "h2d_bytes_per_step": int(8 * nmat * S.nao_of(s["shells"]) ** 2),
@@ -306,6 +344,100 @@ def jk_sph_bench(args):
     print(json.dumps(line))
 
 
+def batch_bench(args):
+    """Molecule batch: 256 molecules of 4..40 atoms (each in a cube of side
+    2.5 n^(1/3), min separation 1.6), spherical s,s,p,p,d,f,g of 3 primitives
+    0.1*2.4^k, one density each (nocc = nao/4), tau 1e-11.  A step is one J/K
+    build of every molecule (plus the density-direct gradient when the
+    gradient classes of g shells are compiled), every angular class of every
+    molecule in one persistent launch, replayed from a CUDA graph.  value =
+    molecules per second of graph device time (FP32-mixed); e2e = the same
+    through the C ABI with host buffers (the densities up, J and K down)."""
+    import torch
+
+    torch.cuda.set_device(0)
+    import integral_b200 as ib
+    from integral_b200 import systems as S
+
+    sysb = S.molecule_batch()
+    mols = sysb["molecules"]
+    thr = 1e-11
+    t0 = time.perf_counter()
+    batch = ib.MoleculeBatch([m["shells"] for m in mols])
+    setup_s = time.perf_counter() - t0
+    dens = [m["dens"] for m in mols]
+    want_grad = False
+    try:
+        batch.jk_grad(dens, thr, precision=0, gradient=True)
+        want_grad = True
+    except ib.IntegralError as e:
+        if e.code != -11:
+            raise
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float64, device="cuda")
+
+    def timed(prec):
+        for _ in range(args.warmup):
+            batch.jk_grad(dens, thr, precision=prec, gradient=want_grad)
+        ms, wall, q, launches, out = 0.0, 0.0, 0, 0, None
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            out = batch.jk_grad(dens, thr, precision=prec, gradient=want_grad)
+            wall += time.perf_counter() - t
+            st = batch.last_stats()
+            ms += st["kernel_ms"]
+            q += st["quartets"]
+            launches += st["launches"]
+        return ms, wall, q, launches, out, batch.last_stats()
+
+    clk = ClockSampler(0)
+    clk.start()
+    ms32, w32, q32, l32, out32, st32 = timed(1)
+    clocks = clk.stop()
+    ms64, w64, q64, _, out64, _ = timed(0)
+    dE = [0.5 * float(np.sum(D * ((a - c) - 0.5 * (b - d))))
+          for D, a, b, c, d in zip(dens, out32[0], out32[1], out64[0], out64[1])]
+    nmol = len(mols)
+    steps = args.steps
+    h2d = int(8 * sum(D.size for D in dens))
+    # CPU baseline: the oracle's J/K of a seeded sample of molecules on every
+    # host thread, scaled to molecules per second
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_py as O
+    nthreads = os.cpu_count() or 1
+    pick = np.random.default_rng(17).choice(nmol, 3, replace=False)
+    t0 = time.perf_counter()
+    for k in pick:
+        O.OracleBasis(mols[k]["shells"]).direct_jk(dens[k][None], thr, nthreads=nthreads)
+    cpu_s = time.perf_counter() - t0
+    line = {
+        "metric": "molecule batch J/K%s molecules/s (FP32-mixed) on B200" % (" + gradient" if want_grad else ""),
+        "unit": "molecules/s", "value": nmol * steps / (ms32 * 1e-3), "n_gpus": 1, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": ms32 / steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "fp32-mixed (fp64 accumulation)",
+        "data": "synthetic (seeded generator, no data set)",
+        "config": {"workload": "256 molecules, 4..40 atoms, s,s,p,p,d,f,g spherical, 3 primitives, one density "
+                               "each (nocc = nao/4), tau 1e-11, one CUDA graph per step%s"
+                               % ("" if want_grad else "; J/K only (gradient classes of g shells not compiled)"),
+                   "molecules": nmol, "atoms": int(sum(batch.natom(m) for m in range(nmol))),
+                   "nao_total": int(sum(batch.nao(m) for m in range(nmol))), "quartets_per_step": q32 // steps,
+                   "batch_setup_s": setup_s, "l2": "flushed between steps (512 MB write)"},
+        "fp64": {"value": nmol * steps / (ms64 * 1e-3), "unit": "molecules/s", "ms_per_step": ms64 / steps,
+                 "mixed_speedup": ms64 / ms32},
+        "energy_error_mixed_vs_fp64_Eh": {"max_abs": float(np.max(np.abs(dE))), "sum": float(np.sum(dE))},
+        "e2e": {"value": nmol * steps / w32, "unit": "molecules/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 2 * h2d},
+        "clocks": clocks,
+        "gpu_launches": l32,
+        "cpu_baseline": {"value": len(pick) / cpu_s, "unit": "molecules/s", "cores": nthreads, "kind": "port",
+                         "sample": "J/K of %d seeded molecules (%s atoms, %.1f s), all threads; %s"
+                                   % (len(pick), ",".join(str(batch.natom(int(k))) for k in pick), cpu_s,
+                                      CPU_KIND)},
+    }
+    print(json.dumps(line))
+
+
 def profile_case(workload="jk"):
     """One mixed J/K build of a 24-atom cut of the bench recipe (12-bohr
     cube): every class of the bench, inputs larger than L2 are not needed
@@ -438,6 +570,17 @@ def cpu_plan(system):
     return B
 
 
+CPU_KIND = ("C++ restatement of the reference CPU path (the Rust crate cannot be built in this image): its generic "
+            "m-marching OS/HGP VRR and Rys engines, not the reference's monomorphised contract_class kernels, so it "
+            "likely understates the reference's own speed")
+
+
+def cpu_sample_size(args, nthreads):
+    """Bra pairs per CPU sample: four per host thread (the bra pair is the
+    work grain), and at least --cpu-sample-bras."""
+    return max(4 * nthreads, args.cpu_sample_bras)
+
+
 def cpu_rate(B, system, nbras, seed, nthreads):
     """Screened quartets/s of the C++ restatement of the reference CPU path
     (bra pair as the grain, one workspace and private J/K per worker) over a
@@ -458,23 +601,27 @@ def reference_arm(args):
     from integral_b200 import systems as S
     system = S.jk_system()
     nthreads = os.cpu_count() or 1
-    rates = []
+    nbras = cpu_sample_size(args, nthreads)
     B = cpu_plan(system)
+    cnt_sum, dt_sum = 0, 0.0
     for step in range(args.warmup + args.steps):
-        r, cnt, dt, nb = cpu_rate(B, system, max(4, args.cpu_sample_bras // 3), 1000 + step, nthreads)
+        # warm-up steps touch a small sample; every timed step draws its own
+        # seeded sample of the same size as the GPU arm's cpu_baseline
+        r, cnt, dt, nb = cpu_rate(B, system, nbras if step >= args.warmup else nthreads, 1000 + step, nthreads)
         if step >= args.warmup:
-            rates.append(r)
-    val = float(statistics.mean(rates))
+            cnt_sum += cnt
+            dt_sum += dt
+    val = cnt_sum / dt_sum
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "strong",
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt_sum / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": {"workload": "direct J/K, 64 atoms, nao 960, 4 densities, tau 1e-12", "nao": 960,
                    "ndens": 4, "threshold": 1e-12},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": nthreads, "kind": "port",
-                         "sample": "%d seeded canonical bra pairs per step (of 73920), all threads; C++ "
-                                   "restatement of the reference CPU path (Rust toolchain absent)"
-                                   % max(4, args.cpu_sample_bras // 3)},
+                         "sample": "%d seeded canonical bra pairs per timed step (of 73920, %d screened quartets "
+                                   "in all), all threads; %s" % (nbras, cnt_sum, CPU_KIND)},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -493,6 +640,8 @@ def main():
         return dense_bench(args)
     if args.workload == "jk-sph":
         return jk_sph_bench(args)
+    if args.workload == "batch":
+        return batch_bench(args)
     if args.impl == "reference":
         return reference_arm(args)
     import torch
@@ -571,6 +720,20 @@ def main():
     sampler = ClockSampler(local) if rank == 0 else None
     t_mixed, q_mixed, l_mixed, prof_mixed, clocks = timed(1, args.warmup, args.steps, sampler)
     Jm, Km = J.cpu().numpy().copy(), K.cpu().numpy().copy()
+    # an SCF caller passes a new density every iteration: time the mixed call
+    # (host wall, synchronous) on a perturbed density against the same call
+    # on the density whose task lists are cached
+    def wall_call(Dx):
+        J.zero_()
+        K.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dc.jk_device(Dx.data_ptr(), nd, J.data_ptr(), K.data_ptr(), thr, True, 1, bras=bras,
+                     stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3
+    wall_same = wall_call(D)
+    wall_new = wall_call((D * 0.999).contiguous())
     t_64, q_64, l_64, prof_64, _ = timed(0, 1, args.steps)
     J64, K64 = J.cpu().numpy(), K.cpu().numpy()
     Dn = system["dens"]
@@ -633,10 +796,12 @@ def main():
 
     cpu = None
     if world == 1:
-        r, cnt, dt, nb = cpu_rate(cpu_plan(system), system, args.cpu_sample_bras, 7, os.cpu_count() or 1)
-        cpu = {"value": r, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
-               "sample": "%d seeded canonical bra pairs of 73920 (%d screened quartets, %.1f s), all threads; "
-                         "C++ restatement of the reference CPU path" % (nb, cnt, dt)}
+        nthreads = os.cpu_count() or 1
+        r, cnt, dt, nb = cpu_rate(cpu_plan(system), system, cpu_sample_size(args, nthreads), 1000 + args.warmup,
+                                  nthreads)
+        cpu = {"value": r, "unit": UNIT, "cores": nthreads, "kind": "port",
+               "sample": "%d seeded canonical bra pairs of 73920 (%d screened quartets, %.1f s), all threads; %s"
+                         % (nb, cnt, dt, CPU_KIND)}
 
     steps = args.steps
     line = {
@@ -659,6 +824,9 @@ def main():
                    "l2": "flushed between steps (512 MB write)"},
         "fp64": {"value": q_64 / (t_64 * 1e-3), "unit": UNIT, "ms_per_step": t_64 / steps,
                  "mixed_speedup": (t_64 / t_mixed), "energy_error_mixed_vs_fp64_Eh": dE},
+        "scf_new_density": {"wall_ms": wall_new, "wall_ms_cached_density": wall_same,
+                            "note": "mixed build on a density 0.999 x the bench's (a new SCF iteration): the "
+                                    "task lists follow the binade of max|D| and are reused"},
         "e2e": {"value": q_mixed / te if te > 0 else None, "unit": UNIT,
                 "h2d_bytes_per_step": int(Dh.numel() * 8), "d2h_bytes_per_step": int(2 * Jh.numel() * 8)},
         "roofline": {"bound": "fp32" if top["fp32"] else "fp64",

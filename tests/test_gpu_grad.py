@@ -148,3 +148,52 @@ def test_grad_error_codes():
     with pytest.raises(ib.IntegralError) as e:
         gc.accumulate_bra_pairs(ib.DirectGradWorkspace(), None, dens, 1e-12, out, precision=7)
     assert e.value.code == -1
+
+
+def test_grad_finite_difference_full_size_12_coordinates():
+    """The 100-atom, nao 1400 gradient system at tau 1e-12: the FP64 GPU
+    gradient against central differences (h = 1e-4 bohr) of the GPU energy
+    E = 1/2 tr(D J) - 1/4 tr(D K) on 12 seeded (atom, axis) coordinates.
+
+    Only quartets with a shell on the moved atom A depend on R_A.  With A's
+    shells placed last (the energy and gradient do not depend on the shell
+    order; D is permuted with the AOs), a canonical quartet (ij|kl) contains
+    a shell of A exactly when its largest index i does, so the bra pairs
+    (i, j) with i on A give both E_A(R_A +- h), whose difference is that of
+    the full energies, and the complete gradient row of A."""
+    s = S.grad_system()
+    shells, D = s["shells"], s["dens"]
+    nf = [S.n_func(sh["l"], False) for sh in shells]
+    offs = np.concatenate([[0], np.cumsum(nf)])
+    centers = [tuple(sh["center"]) for sh in shells]
+    atoms = list(dict.fromkeys(centers))
+    rng = np.random.default_rng(2024)
+    picks = [(int(rng.integers(len(atoms))), int(rng.integers(3))) for _ in range(12)]
+    h = 1e-4
+    for a, x in picks:
+        on_a = [k for k, c in enumerate(centers) if c == atoms[a]]
+        order = [k for k in range(len(shells)) if k not in on_a] + on_a
+        ao = np.concatenate([np.arange(offs[k], offs[k + 1]) for k in order])
+        Dp = np.ascontiguousarray(D[np.ix_(ao, ao)])
+        first = len(shells) - len(on_a)
+        bras = np.array([i * (i + 1) // 2 + j for i in range(first, len(shells)) for j in range(i + 1)])
+
+        def placed(delta):
+            out = []
+            for k in order:
+                sh = dict(shells[k])
+                if k in on_a:
+                    c = list(sh["center"])
+                    c[x] += delta
+                    sh["center"] = c
+                out.append(sh)
+            return out
+
+        def energy(delta):
+            J, K = ib.Basis(placed(delta)).direct_contractor().jk(Dp[None], s["threshold"], bras=bras)
+            return 0.5 * float(np.sum(Dp * J[0])) - 0.25 * float(np.sum(Dp * K[0]))
+
+        fd = (energy(h) - energy(-h)) / (2 * h)
+        g, _ = gpu_grad(placed(0.0), [(0.5, Dp, Dp)], [(-0.25, Dp, Dp)], s["threshold"], bras=bras)
+        moved_row = len(atoms) - 1  # A's centre appears last in the reordered basis
+        assert abs(fd - g[moved_row, x]) < 1e-6, (a, x, fd, g[moved_row, x])

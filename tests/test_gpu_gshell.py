@@ -1,0 +1,84 @@
+"""GPU parity of the g-shell classes (l = 4, the highest shell of the
+molecule-batch workload) against the oracle: the dense tensor and single
+(gg|gg) blocks, Cartesian and spherical, within the dense-ERI contract, and
+direct J/K with the exact screened quartet list; the gradient of a basis
+with g shells is reported unsupported (its classes are not compiled)."""
+import numpy as np
+import pytest
+
+import integral_b200 as ib
+import oracle_py as O
+from integral_b200 import systems as S
+
+pytestmark = pytest.mark.gpu
+
+
+def check_eri(gpu, ref):
+    peak = float(np.max(np.abs(ref)))
+    d = np.abs(gpu - ref)
+    sig = np.abs(ref) >= 1e-3 * peak
+    assert float(np.max(d[sig] / np.abs(ref[sig]))) < 1e-12
+    assert float(np.max(d)) < 1e-13 * max(peak, 1.0)
+
+
+def two_centre_g(spherical):
+    """s, d, g on one centre and p, g on another (2 primitives each)."""
+    rng = np.random.default_rng(41)
+    out = []
+    for centre, letters in (([0.0, 0.0, 0.0], "sdg"), ([0.7, -0.4, 1.1], "pg")):
+        for k, letter in enumerate(letters):
+            exps = [0.9 * 2.5 ** j * (1.0 + 0.1 * k) for j in range(2)]
+            out.append(dict(l=S.L_OF[letter], spherical=spherical, center=centre, exps=exps,
+                            coefs=[float(x) for x in rng.uniform(0.3, 1.0, 2)]))
+    return out
+
+
+@pytest.mark.parametrize("spherical", [False, True], ids=["cart", "sph"])
+def test_dense_eri_with_g_shells(spherical):
+    shells = two_centre_g(spherical)
+    check_eri(ib.Basis(shells).eri(), O.OracleBasis(shells).eri())
+
+
+@pytest.mark.parametrize("spherical", [False, True], ids=["cart", "sph"])
+def test_gggg_block(spherical):
+    shells = two_centre_g(spherical)
+    B, OB = ib.Basis(shells), O.OracleBasis(shells)
+    for q in [(2, 4, 2, 4), (4, 4, 4, 4), (2, 2, 4, 2), (4, 0, 2, 3)]:
+        check_eri(B.eri_block(*q), OB.eri_block(*q).reshape(-1))
+
+
+def molecule(natom, seed):
+    """One molecule of the batch recipe: spherical s,s,p,p,d,f,g of 3
+    primitives 0.1*2.4^k in a cube of side 2.5 n^(1/3)."""
+    rng = np.random.default_rng(seed)
+    centers = S.place_atoms(rng, natom, 2.5 * natom ** (1.0 / 3.0), 1.6)
+    shells = S.build_shells(rng, centers, "ssppdfg", 3, 0.1, 2.4, 0.2, 1.0, spherical=True)
+    D = S.densities(rng, S.nao_of(shells), max(1, S.nao_of(shells) // 4), 1)
+    return shells, D
+
+
+def test_jk_with_g_shells_exact_list():
+    shells, D = molecule(3, 7)
+    dc = ib.Basis(shells).direct_contractor()
+    J, K = dc.jk(D, 1e-11)
+    st = dc.last_stats()
+    Jo, Ko, cnt, hsh = O.OracleBasis(shells).direct_jk(D, 1e-11, nthreads=16)
+    assert st["quartets"] == cnt and st["quartet_hash"] == hsh
+    assert float(np.max(np.abs(J - Jo))) < 1e-12 * float(np.max(np.abs(Jo)))
+    assert float(np.max(np.abs(K - Ko))) < 1e-12 * float(np.max(np.abs(Ko)))
+    Jm, Km = dc.jk(D, 1e-11, precision=1)
+    e = lambda Jx, Kx: 0.5 * float(np.sum(D[0] * (Jx[0] - 0.5 * Kx[0])))
+    assert abs(e(Jm, Km) - e(J, K)) < 1e-7
+
+
+def test_gradient_of_g_shells_is_reported_unsupported():
+    """The gradient classes stop at f (their raised tables reach l = 4); a
+    basis with g shells gets IGPU_ERR_UNSUPPORTED, never a wrong result."""
+    shells, D = molecule(2, 8)
+    gc = ib.Basis(shells).direct_grad_contractor()
+    dens = gc.density([ib.GradDensityTerm(0.5, D[0], D[0])], [ib.GradDensityTerm(-0.25, D[0], D[0])])
+    out = np.zeros((gc.natom(), 3))
+    with pytest.raises(ib.IntegralError) as e:
+        gc.accumulate_bra_pairs(ib.DirectGradWorkspace(), None, dens, 1e-11, out)
+    assert e.value.code == -11 and "gradient classes" in str(e.value)
+    assert np.all(out == 0.0)

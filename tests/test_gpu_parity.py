@@ -82,14 +82,27 @@ def test_eri_builder_matches_dense():
     assert float(np.max(np.abs(O4[rows] - R4[rows]))) < 1e-13 * float(np.max(np.abs(ref)))
 
 
-def test_schwarz_bounds_match_oracle():
-    s = S.jk_system(natom=8, side=8.0)
-    B = ib.Basis(s["shells"])
-    q = B.schwarz_bounds().reshape(len(s["shells"]), -1)
-    qo = O.OracleBasis(s["shells"]).schwarz()
-    lo = np.tril(np.ones_like(q, dtype=bool))
-    # Q = sqrt(max diagonal integral): within the 1e-12 ERI contract
-    assert float(np.max(np.abs(q[lo] - qo[lo]) / np.maximum(qo[lo], 1e-300))) < 1e-12
+@pytest.mark.parametrize("system", ["jk-8atom", "jk-64atom", "grad-100atom", "sph-f-6atom"])
+def test_schwarz_bounds_are_the_reference_bit_for_bit(system):
+    """The plan screens with the reference's own Schwarz bounds, bit for bit
+    (every pair of these contracted bases is an OS/HGP diagonal under the
+    Auto policy), so the screened quartet lists match by construction."""
+    shells = {"jk-8atom": lambda: S.jk_system(natom=8, side=8.0)["shells"],
+              "jk-64atom": lambda: S.jk_system()["shells"],
+              "grad-100atom": lambda: S.grad_system()["shells"],
+              "sph-f-6atom": lambda: S.jk_spherical_system(natom=6, side=9.0)["shells"]}[system]()
+    q = ib.Basis(shells).schwarz_bounds().reshape(len(shells), -1)
+    qo = O.OracleBasis(shells).schwarz()
+    assert q.view(np.uint64).tolist() == qo.view(np.uint64).tolist()
+
+
+def test_schwarz_bounds_of_rys_pairs_within_the_eri_contract():
+    """Pairs the Auto policy evaluates with Rys (single primitives, the
+    reference's extended gradient fixture) keep the device evaluation."""
+    shells = S.grad_extended_fixture()
+    q = ib.Basis(shells).schwarz_bounds().reshape(len(shells), -1)
+    qo = O.OracleBasis(shells).schwarz()
+    assert float(np.max(np.abs(q - qo) / np.maximum(qo, 1e-300))) < 1e-12
 
 
 @pytest.mark.parametrize("spherical", [False, True], ids=["cart", "sph"])

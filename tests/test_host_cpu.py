@@ -59,6 +59,22 @@ def test_plan_create_validation_codes():
     assert b"NULL" in L.igpu_last_error_string()
 
 
+def test_batch_create_validation_codes():
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    s, keep = _shell()
+    counts = (ctypes.c_size_t * 2)(1, 0)
+    assert L.igpu_batch_create(ctypes.byref(s), counts, 0, ctypes.byref(h)) == -1   # no molecules
+    assert L.igpu_batch_create(ctypes.byref(s), counts, 2, ctypes.byref(h)) == -1   # molecule without shells
+    one = (ctypes.c_size_t * 1)(1)
+    bad, keep2 = _shell(nprim=0)
+    assert L.igpu_batch_create(ctypes.byref(bad), one, 1, ctypes.byref(h)) == -2    # EmptyContraction
+    bad, keep3 = _shell(l=7)
+    assert L.igpu_batch_create(ctypes.byref(bad), one, 1, ctypes.byref(h)) == -4    # AngularMomentumTooHigh
+    assert L.igpu_batch_create(ctypes.byref(s), one, 1, None) == -1
+    assert L.igpu_batch_destroy(None) == 0
+
+
 def test_ctypes_structs_match_the_header_layout(tmp_path):
     """Every struct of include/integral_gpu.h, compiled by the host C
     compiler, has the size and field offsets of its ctypes mirror."""
