@@ -299,19 +299,22 @@ int igpu_last_stats(const igpu_plan* plan, igpu_stats* stats);
 /* Per-launch records of the last J/K or gradient call (*n = count; at most
  * cap written to out). */
 int igpu_last_profile(const igpu_plan* plan, igpu_launch_record* out, size_t cap, size_t* n);
-/* Chunk autotuner for the J/K launches (no counterpart in the reference,
- * whose CPU path has no launch shapes to tune).  Runs the J/K build of
- * d_dens (device, ndens x nao x nao) at `threshold` and `precision` once
- * per candidate chunk (4, 8, 16, 32 or 64 tasks per team per grab), twice
- * over, into scratch outputs it allocates, and keeps per angular class and
- * precision the chunk of the shortest launch.  Later J/K calls on the plan
- * use the kept chunks (16 before any tuning); results differ only in the
- * order of the atomic additions.  Costs ten J/K builds. */
+/* Launch-shape autotuner for the J/K launches (no counterpart in the
+ * reference, whose CPU path has no launch shapes to tune).  Runs the J/K
+ * build of d_dens (device, ndens x nao x nao) at `threshold` and `precision`
+ * into scratch outputs it allocates, in two stages, each candidate twice:
+ * first per candidate chunk (4, 8, 16, 32 or 64 tasks per team per grab,
+ * i.e. quartets per warp per grab), then, with the chosen chunks, per cap on
+ * the persistent grid (1, 2, 3 or 4 blocks per SM, or the occupancy limit).
+ * It keeps per angular class and precision the candidate of the shortest
+ * launch; later J/K calls on the plan use them (16 and the occupancy limit
+ * before any tuning).  Results differ only in the order of the atomic
+ * additions.  Costs twenty J/K builds. */
 int igpu_autotune_jk(igpu_plan* plan, const double* d_dens, int ndens, double threshold, int precision,
                      void* stream);
-/* The same chunk autotuner for the gradient launches: ten igpu_grad calls
- * on the given (host) term matrices, at threshold and precision, into a
- * scratch output; later gradient calls on the plan use the kept chunks. */
+/* The same two-stage autotuner for the gradient launches: twenty igpu_grad
+ * calls on the given (host) term matrices, at threshold and precision, into
+ * a scratch output; later gradient calls on the plan use the kept shapes. */
 int igpu_autotune_grad(igpu_plan* plan, const igpu_term* coulomb, int ncoul, const igpu_term* exchange,
                        int nexch, double threshold, int precision);
 

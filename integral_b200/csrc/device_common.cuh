@@ -341,22 +341,50 @@ __device__ __forceinline__ void rys_root_fp64(double T, int r, double& x, double
   w = chebev<double>(base + RYS_NC, xi);
 }
 
-// Where the FP32 launches generate roots and weights in FP64: every
-// quadrature of five or more roots (high angular momentum,
-// l_a + l_b + l_c + l_d >= 8), and T in the last two Chebyshev subintervals
-// below the asymptotic crossover, where the Clenshaw sums lose digits (the
-// reference's own FP64 weights lose three to four there, src/math/rys.rs:
-// 80-89).  Above the crossover the roots and weights are the closed forms
-// c_i / T and w_i T^{-1/2}, exact to FP32 rounding.
+// The FP32 launches generate roots and weights in FP64 for every quadrature
+// of five or more roots (high angular momentum, l_a + l_b + l_c + l_d >= 8):
+// the n where Clenshaw sums lose digits just below the asymptotic crossover
+// (the reference's own FP64 weights lose three to four there at n = 9, 11,
+// 13, src/math/rys.rs:80-89) are all among them.  Above the crossover the
+// roots and weights are the closed forms c_i / T and w_i T^{-1/2}, exact to
+// FP32 rounding at every n.
 constexpr int ROOTS64_NR = 5;
 template <int N, typename R>
-__device__ __forceinline__ bool roots_in_fp64(R T) {
-  if constexpr (sizeof(R) == 8) {
-    return false;
-  } else {
-    const RysMeta m = c_rys[N];
-    return N >= ROOTS64_NR || (T < R(m.t_hi) && T >= R(m.t_hi - 2.0 * m.width));
+__device__ __forceinline__ bool roots_in_fp64(R) {
+  return sizeof(R) == 4 && N >= ROOTS64_NR;
+}
+
+// quartet_header for the FP32 launches from the FP32 pair copies; ac = the
+// bra's first evaluation shell centre minus the ket's, rounded once per
+// quartet.
+__device__ __forceinline__ QuartetHdr<float> quartet_header_f(const PrimPairF& bp, const PrimPairF& kp, float acx,
+                                                              float acy, float acz, double omega) {
+  QuartetHdr<float> h;
+  const float p = bp.zeta, q = kp.zeta;
+  h.p = p;
+  h.q = q;
+  h.pq = p + q;
+  const float rho = p * q / h.pq;
+  h.pqx = acx + (bp.pax - kp.pax);
+  h.pqy = acy + (bp.pay - kp.pay);
+  h.pqz = acz + (bp.paz - kp.paz);
+  h.T = rho * (h.pqx * h.pqx + h.pqy * h.pqy + h.pqz * h.pqz);
+  h.pref = 34.98683665524972f / (p * q * sqrtf(h.pq)) * bp.e * kp.e;
+  h.pax = bp.pax;
+  h.pay = bp.pay;
+  h.paz = bp.paz;
+  h.qcx = kp.pax;
+  h.qcy = kp.pay;
+  h.qcz = kp.paz;
+  h.xs = 1.f;
+  if (omega > 0.0) {
+    const float w2 = float(omega) * float(omega);
+    const float sc = w2 / (rho + w2);
+    h.T *= sc;
+    h.pref *= sqrtf(sc);
+    h.xs = sc;
   }
+  return h;
 }
 
 // ----------------------------------------------------------- misc device

@@ -1,7 +1,9 @@
-// Gradient kernels of one bra pair class: compiled once per PCB (with
-// -DPCB=<n>, pair class pc = l_a(l_a+1)/2 + l_b of the evaluation bra), it
-// instantiates the FP64 and FP32 gradient kernels of every ket class
-// pck <= PCB and exports their registration and its module constants.
+// Gradient kernels of one bra pair class: compiled with -DPCB=<n> (pair
+// class pc = l_a(l_a+1)/2 + l_b of the evaluation bra), it instantiates the
+// FP64 and FP32 gradient kernels of every ket class pck <= PCB, or, with
+// -DPCK=<k> as well, of ket class k alone (the build splits the largest bra
+// classes that way), and adds their registration and its module constants
+// to the registry at load time.
 #include <utility>
 
 #include "grad_kernel.cuh"
@@ -10,16 +12,20 @@
 #ifndef PCB
 #error "compile with -DPCB=<bra pair class>"
 #endif
-
-#define IGPU_CAT2(a, b) a##b
-#define IGPU_CAT(a, b) IGPU_CAT2(a, b)
+#ifdef PCK
+#define PCK_LO PCK
+#define PCK_HI PCK
+#else
+#define PCK_LO 0
+#define PCK_HI PCB
+#endif
 
 namespace igpu {
 namespace {
 
-template <int PCK>
+template <int K>
 void register_one(KernelEntry* tab, int npc) {
-  constexpr int LA = pc_la(PCB), LB = pc_lb(PCB), LC = pc_la(PCK), LD = pc_lb(PCK);
+  constexpr int LA = pc_la(PCB), LB = pc_lb(PCB), LC = pc_la(K), LD = pc_lb(K);
   using G64 = GradShape<LA, LB, LC, LD, double>;
   using G32 = GradShape<LA, LB, LC, LD, float>;
   KernelEntry e;
@@ -30,20 +36,21 @@ void register_one(KernelEntry* tab, int npc) {
   e.smem32 = (128 / G32::T) * G32::SMEM_PER_TEAM * (int)sizeof(float);
   e.slot = grad_slot_layout(LA, LB, LC, LD).total;
   e.valid = true;
-  tab[PCB * npc + PCK] = e;
+  tab[PCB * npc + K] = e;
 }
 
 template <int... I>
 void register_all(KernelEntry* tab, int npc, std::integer_sequence<int, I...>) {
-  (register_one<I>(tab, npc), ...);
+  (register_one<PCK_LO + I>(tab, npc), ...);
 }
+
+void register_unit(KernelEntry* tab, int npc) {
+  register_all(tab, npc, std::make_integer_sequence<int, PCK_HI - PCK_LO + 1>{});
+}
+
+cudaError_t upload_unit(const ConstData& c) { return upload_module_constants(c); }
+
+const int g_added = add_class_unit(true, register_unit, upload_unit);
 
 }  // namespace
-
-void IGPU_CAT(register_grad_classes_, PCB)(KernelEntry* tab, int npc) {
-  register_all(tab, npc, std::make_integer_sequence<int, PCB + 1>{});
-}
-
-cudaError_t IGPU_CAT(upload_grad_constants_, PCB)(const ConstData& c) { return upload_module_constants(c); }
-
 }  // namespace igpu

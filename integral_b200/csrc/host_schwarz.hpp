@@ -1,9 +1,12 @@
-// Exact Schwarz bounds on the host (host_schwarz.cpp): the diagonal quartets
-// (ij|ij) evaluated with the reference's arithmetic, bit for bit, wherever its
-// Auto engine policy picks Obara-Saika / Head-Gordon-Pople.
+// Exact Schwarz bounds (host_schwarz.cpp on the host, schwarz_dev.cu on the
+// device, both running schwarz_core.cuh): the diagonal quartets (ij|ij)
+// evaluated with the reference's arithmetic, bit for bit, wherever its Auto
+// engine policy picks Obara-Saika / Head-Gordon-Pople.
 #pragma once
 #include <utility>
 #include <vector>
+
+#include "schwarz_core.cuh"
 
 namespace igpu {
 
@@ -32,5 +35,15 @@ bool schwarz_exact(const SchwarzShell& si, const SchwarzShell& sj, double& q);
 // threads (<= 0: all hardware threads); done[x] = 1 where q[x] was set.
 void schwarz_exact_many(const std::vector<SchwarzShell>& shells, const std::vector<std::pair<int, int>>& pairs,
                         std::vector<double>& q, std::vector<unsigned char>& done, int nthreads);
+
+// Inputs of the shared evaluation (schwarz_core.cuh): the Boys table and its
+// constants (host pointers), the work-array layout of the class (li, lj) for
+// at most maxpp primitive pairs (eoff receives the e-offset table the
+// layout's eoff must point to), and the kappa of every primitive
+// combination of (si, sj), si outer.
+sc::BoysDev schwarz_boys_view();
+const std::vector<double>& schwarz_boys_table();
+sc::SClass schwarz_class_layout(int li, int lj, int maxpp, std::vector<int>& eoff);
+void schwarz_kappa(const SchwarzShell& si, const SchwarzShell& sj, double* out);
 
 }  // namespace igpu

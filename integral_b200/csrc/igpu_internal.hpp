@@ -39,6 +39,18 @@ struct PrimPairD {
   double e;          // kappa * c_A * c_B (effective coefficients)
 };
 
+// FP32 copy of one primitive pair for the FP32 launches, rounded once at
+// plan creation: the FP32 header then needs no double loads or conversions.
+// P - Q of a quartet is formed as (A - C) + (PA - QC), with A - C (the
+// evaluation shells' centres) rounded once per quartet, so no absolute
+// coordinate enters an FP32 difference.
+struct PrimPairF {
+  float zeta, e;
+  float pax, pay, paz;
+  float alpha, beta;
+  float pad;
+};
+
 // One canonical shell pair (i >= j in the reference's sense) with its
 // evaluation orientation.  An auxiliary pair of density fitting (an aux shell
 // with the unit s dummy, src/df.rs:1-37) has i = the aux shell's position in
@@ -148,6 +160,7 @@ struct KernelArgs {
   const DevShell* shells;
   const PairD* pairs;
   const PrimPairD* prims;
+  const PrimPairF* primsf;  // FP32 copy of prims (same order)
   const double* c2s;     // c2s matrices (ratio folded), c2s_off[l] into it
   int c2s_off[GPU_MAX_L + 3];
   int nsh;

@@ -5,111 +5,31 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <vector>
 
 #include "launch.hpp"
 
 namespace igpu {
 
 constexpr int NPC = (KERNEL_MAX_L + 1) * (KERNEL_MAX_L + 2) / 2;
-
-#define IGPU_DECL(n)                                     \
-  void register_classes_##n(KernelEntry* tab, int npc); \
-  cudaError_t upload_constants_##n(const ConstData& c);
-IGPU_DECL(0)
-IGPU_DECL(1)
-IGPU_DECL(2)
-IGPU_DECL(3)
-IGPU_DECL(4)
-IGPU_DECL(5)
-#if KERNEL_MAX_L >= 3
-IGPU_DECL(6)
-IGPU_DECL(7)
-IGPU_DECL(8)
-IGPU_DECL(9)
-#endif
-#if KERNEL_MAX_L >= 4
-IGPU_DECL(10)
-IGPU_DECL(11)
-IGPU_DECL(12)
-IGPU_DECL(13)
-IGPU_DECL(14)
-#endif
-
-#define IGPU_GDECL(n)                                         \
-  void register_grad_classes_##n(KernelEntry* tab, int npc); \
-  cudaError_t upload_grad_constants_##n(const ConstData& c);
-IGPU_GDECL(0)
-IGPU_GDECL(1)
-IGPU_GDECL(2)
-#if GRAD_KERNEL_MAX_L >= 2
-IGPU_GDECL(3)
-IGPU_GDECL(4)
-IGPU_GDECL(5)
-#endif
-#if GRAD_KERNEL_MAX_L >= 3
-IGPU_GDECL(6)
-IGPU_GDECL(7)
-IGPU_GDECL(8)
-IGPU_GDECL(9)
-#endif
-#if GRAD_KERNEL_MAX_L >= 4
-IGPU_GDECL(10)
-IGPU_GDECL(11)
-IGPU_GDECL(12)
-IGPU_GDECL(13)
-IGPU_GDECL(14)
-#endif
-
-using RegFn = void (*)(KernelEntry*, int);
-using UpFn = cudaError_t (*)(const ConstData&);
-static const RegFn k_reg[NPC] = {
-    register_classes_0, register_classes_1, register_classes_2, register_classes_3, register_classes_4,
-    register_classes_5,
-#if KERNEL_MAX_L >= 3
-    register_classes_6, register_classes_7, register_classes_8, register_classes_9,
-#endif
-#if KERNEL_MAX_L >= 4
-    register_classes_10, register_classes_11, register_classes_12, register_classes_13, register_classes_14,
-#endif
-};
-static const UpFn k_up[NPC] = {
-    upload_constants_0, upload_constants_1, upload_constants_2, upload_constants_3, upload_constants_4,
-    upload_constants_5,
-#if KERNEL_MAX_L >= 3
-    upload_constants_6, upload_constants_7, upload_constants_8, upload_constants_9,
-#endif
-#if KERNEL_MAX_L >= 4
-    upload_constants_10, upload_constants_11, upload_constants_12, upload_constants_13, upload_constants_14,
-#endif
-};
-
 constexpr int GNPC = (GRAD_KERNEL_MAX_L + 1) * (GRAD_KERNEL_MAX_L + 2) / 2;
-static const RegFn g_reg[GNPC] = {
-    register_grad_classes_0, register_grad_classes_1, register_grad_classes_2,
-#if GRAD_KERNEL_MAX_L >= 2
-    register_grad_classes_3, register_grad_classes_4, register_grad_classes_5,
-#endif
-#if GRAD_KERNEL_MAX_L >= 3
-    register_grad_classes_6, register_grad_classes_7, register_grad_classes_8, register_grad_classes_9,
-#endif
-#if GRAD_KERNEL_MAX_L >= 4
-    register_grad_classes_10, register_grad_classes_11, register_grad_classes_12, register_grad_classes_13,
-    register_grad_classes_14,
-#endif
+
+namespace {
+struct ClassUnit {
+  bool grad;
+  ClassRegFn reg;
+  ConstUpFn up;
 };
-static const UpFn g_up[GNPC] = {
-    upload_grad_constants_0, upload_grad_constants_1, upload_grad_constants_2,
-#if GRAD_KERNEL_MAX_L >= 2
-    upload_grad_constants_3, upload_grad_constants_4, upload_grad_constants_5,
-#endif
-#if GRAD_KERNEL_MAX_L >= 3
-    upload_grad_constants_6, upload_grad_constants_7, upload_grad_constants_8, upload_grad_constants_9,
-#endif
-#if GRAD_KERNEL_MAX_L >= 4
-    upload_grad_constants_10, upload_grad_constants_11, upload_grad_constants_12, upload_grad_constants_13,
-    upload_grad_constants_14,
-#endif
-};
+std::vector<ClassUnit>& class_units() {
+  static std::vector<ClassUnit> v;
+  return v;
+}
+}  // namespace
+
+int add_class_unit(bool grad, ClassRegFn reg, ConstUpFn up) {
+  class_units().push_back({grad, reg, up});
+  return (int)class_units().size();
+}
 
 static KernelEntry g_table[NPC * NPC];
 static KernelEntry g_grad_table[GNPC * GNPC];
@@ -128,7 +48,8 @@ static void set_smem_limits(KernelEntry* tab, int n) {
 
 const KernelEntry* grad_entry(int pcb, int pck) {
   std::call_once(g_grad_once, [] {
-    for (int b = 0; b < GNPC; ++b) g_reg[b](g_grad_table, GNPC);
+    for (const ClassUnit& u : class_units())
+      if (u.grad) u.reg(g_grad_table, GNPC);
     set_smem_limits(g_grad_table, GNPC * GNPC);
   });
   if (pcb < 0 || pck < 0 || pcb >= GNPC || pck >= GNPC || pcb < pck) return nullptr;
@@ -138,7 +59,8 @@ const KernelEntry* grad_entry(int pcb, int pck) {
 
 const KernelEntry* kernel_entry(int pcb, int pck) {
   std::call_once(g_once, [] {
-    for (int b = 0; b < NPC; ++b) k_reg[b](g_table, NPC);
+    for (const ClassUnit& u : class_units())
+      if (!u.grad) u.reg(g_table, NPC);
     set_smem_limits(g_table, NPC * NPC);
   });
   if (pcb < 0 || pck < 0 || pcb >= NPC || pck >= NPC || pcb < pck) return nullptr;
@@ -147,12 +69,8 @@ const KernelEntry* kernel_entry(int pcb, int pck) {
 }
 
 cudaError_t upload_all_constants(const ConstData& c) {
-  for (int b = 0; b < NPC; ++b) {
-    cudaError_t e = k_up[b](c);
-    if (e != cudaSuccess) return e;
-  }
-  for (int b = 0; b < GNPC; ++b) {
-    cudaError_t e = g_up[b](c);
+  for (const ClassUnit& u : class_units()) {
+    cudaError_t e = u.up(c);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

@@ -26,6 +26,14 @@ struct KernelEntry {
 #define GRAD_KERNEL_MAX_L 3
 #endif
 
+// Every class translation unit (class_tu.cu, grad_tu.cu: one per bra pair
+// class, or one per (bra, ket) class for the largest bras) adds itself at
+// load time: `reg` fills its entries of the value or gradient table, `up`
+// uploads the constant tables of its device module.
+using ClassRegFn = void (*)(KernelEntry* tab, int npc);
+using ConstUpFn = cudaError_t (*)(const ConstData&);
+int add_class_unit(bool grad, ClassRegFn reg, ConstUpFn up);
+
 int kernel_npc();
 // Gradient kernel of the class (pcb | pck), same conventions; the entry's
 // slot is the gradient scratch per team.

@@ -73,11 +73,13 @@ static int sm_count() {
   return count[dev];
 }
 
-size_t grid_for(const KernelEntry* e, bool fp32, unsigned long long total) {
+size_t grid_for(const KernelEntry* e, bool fp32, unsigned long long total, int bps_cap) {
   const int nsm = sm_count();
   const int teams_per_block = 128 / e->team;
   const unsigned long long need = (total + teams_per_block - 1) / teams_per_block;
-  const unsigned long long cap = (unsigned long long)blocks_per_sm(e, fp32) * nsm;
+  int bps = blocks_per_sm(e, fp32);
+  if (bps_cap > 0 && bps_cap < bps) bps = bps_cap;
+  const unsigned long long cap = (unsigned long long)bps * nsm;
   return (size_t)std::max<unsigned long long>(1, std::min(need, cap));
 }
 
@@ -87,6 +89,7 @@ KernelArgs base_args(igpu_plan* P) {
   A.shells = P->d_shells.p;
   A.pairs = P->d_pairs.p;
   A.prims = P->d_prims.p;
+  A.primsf = P->d_primsf.p;
   A.c2s = P->d_c2s.p;
   for (int l = 0; l < GPU_MAX_L + 3; ++l) A.c2s_off[l] = P->c2s_off[l];
   A.nsh = P->nsh;
@@ -172,8 +175,9 @@ int tune_key(int pcb, int pck, bool fp32, bool grad) {
   return ((pcb * 64 + pck) * 2 + (fp32 ? 1 : 0)) | (grad ? (1 << 20) : 0);
 }
 
-// Chunk tuning: note every launch time of the last call made at chunk
-// multiplier m, then keep per class the multiplier of the shortest time.
+// Tuning: note every launch time of the last call made with candidate m
+// (a chunk multiplier, or a blocks-per-SM cap), then keep per class the
+// candidate of the shortest time.
 void tune_record(igpu_plan* P, int m, bool grad, std::map<int, std::map<int, float>>& best) {
   for (const igpu_launch_record& r : P->log.profile) {
     auto& slot = best[tune_key(pair_class(r.la, r.lb), pair_class(r.lc, r.ld), r.fp32 != 0, grad)];
@@ -181,17 +185,51 @@ void tune_record(igpu_plan* P, int m, bool grad, std::map<int, std::map<int, flo
     if (it == slot.end() || r.ms < it->second) slot[m] = r.ms;
   }
 }
-void tune_keep(igpu_plan* P, const std::map<int, std::map<int, float>>& best) {
+void tune_keep(igpu_plan* P, const std::map<int, std::map<int, float>>& best, bool bps) {
   for (const auto& kv : best) {
-    int pick = 16;
+    int pick = bps ? 0 : 16;
     float t = std::numeric_limits<float>::infinity();
     for (const auto& mt : kv.second)
       if (mt.second < t) {
         t = mt.second;
         pick = mt.first;
       }
-    P->tuned_mult[kv.first] = pick;
+    if (bps)
+      P->tuned_bps[kv.first] = pick;
+    else
+      P->tuned_mult[kv.first] = pick;
   }
+}
+
+// The two-stage tuner of igpu_autotune_jk / igpu_autotune_grad: `run` makes
+// one build; stage one times every chunk multiplier (tasks a warp claims per
+// grab, in units of its teams) at the occupancy grid, stage two every
+// blocks-per-SM cap of the grid with the chosen chunks; each twice over.
+int tune_two_stage(igpu_plan* P, bool grad, const std::function<int()>& run) {
+  const int mults[] = {4, 8, 16, 32, 64};
+  std::map<int, std::map<int, float>> best;
+  for (int rep = 0; rep < 2; ++rep)
+    for (int m : mults) {
+      P->tune_mult = m;
+      const int rc = run();
+      P->tune_mult = 0;
+      if (rc) return rc;
+      tune_record(P, m, grad, best);
+    }
+  tune_keep(P, best, false);
+  // cap 0 is the occupancy limit itself
+  const int caps[] = {1, 2, 3, 4, 0};
+  std::map<int, std::map<int, float>> best_bps;
+  for (int rep = 0; rep < 2; ++rep)
+    for (int c : caps) {
+      P->tune_bps = c > 0 ? c : -1;
+      const int rc = run();
+      P->tune_bps = 0;
+      if (rc) return rc;
+      tune_record(P, c, grad, best_bps);
+    }
+  tune_keep(P, best_bps, true);
+  return IGPU_OK;
 }
 
 // Scratch doubles per team: the class slot plus, for symmetric J/K, the
@@ -233,7 +271,15 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     Launch* L = ts.launches[li].get();
     if (L->total == 0) continue;
     const KernelEntry* e = entry(L->pcb, L->pck);
-    const size_t grid = grid_for(e, L->fp32, L->total);
+    const int key = tune_key(L->pcb, L->pck, L->fp32, A.mode == MODE_GRAD);
+    int cap = 0;  // blocks-per-SM cap of the grid (0: the occupancy limit)
+    if (P->tune_bps) {
+      cap = P->tune_bps > 0 ? P->tune_bps : 0;
+    } else if (A.mode == MODE_JK || A.mode == MODE_GRAD) {
+      auto t = P->tuned_bps.find(key);
+      if (t != P->tuned_bps.end()) cap = t->second;
+    }
+    const size_t grid = grid_for(e, L->fp32, L->total, cap);
     A.scratch = P->d_scratch.p;
     A.slot_doubles = slot_with_acc(e, L->pcb, A);
     A.acc_offset = e->slot;
@@ -242,7 +288,7 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     if (P->tune_mult) {
       mult = P->tune_mult;
     } else if (A.mode == MODE_JK || A.mode == MODE_GRAD) {
-      auto t = P->tuned_mult.find(tune_key(L->pcb, L->pck, L->fp32, A.mode == MODE_GRAD));
+      auto t = P->tuned_mult.find(key);
       if (t != P->tuned_mult.end()) mult = t->second;
     }
     A.chunk = (unsigned long long)(32 / e->team) * mult;
@@ -255,9 +301,10 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     A.task.total = L->total;
     A.fp32 = L->fp32 ? 1 : 0;
     A.builder_swap = L->builder_swap;
-    CK(cudaEventRecord(lg.events[2 * li], s));
+    // external records, so that a captured graph records them on replay
+    CK(cudaEventRecordWithFlags(lg.events[2 * li], s, cudaEventRecordExternal));
     CK(launch_quartets(e, L->fp32, (int)grid, A, s));
-    CK(cudaEventRecord(lg.events[2 * li + 1], s));
+    CK(cudaEventRecordWithFlags(lg.events[2 * li + 1], s, cudaEventRecordExternal));
     ++launches;
     igpu_launch_record r{};
     r.la = pc_la_host(L->pcb);
@@ -286,7 +333,10 @@ int collect_profile(igpu_plan* P, int ndens, bool jk, int grad_terms_c, int grad
     igpu_launch_record& r = lg.profile[k];
     const size_t li = lg.profile_launch[k];
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, lg.events[2 * li], lg.events[2 * li + 1]);
+    if (cudaEventElapsedTime(&ms, lg.events[2 * li], lg.events[2 * li + 1]) != cudaSuccess) {
+      cudaGetLastError();  // a launch without a usable record: no time, no sticky error
+      ms = 0.f;
+    }
     r.ms = ms;
     r.quartets = c[li].quartets;
     r.prim_quartets = c[li].prim_quartets;
@@ -501,16 +551,104 @@ int run_schwarz(igpu_plan* P) {
   return IGPU_OK;
 }
 
-// Replace the device Q of every canonical pair for which the reference's
-// Auto policy picks OS/HGP by the host's bit-exact evaluation in the
+// The reference's Schwarz bounds of the listed ordered shell pairs (i, j)
+// wherever its Auto policy evaluates (ij|ij) with OS/HGP, on the device with
+// the shared bit-exact evaluation (schwarz_core.cuh): one launch per class
+// (l_i, l_j), one thread per pair.  done[x] = 1 where q[x] was set.
+int exact_schwarz_pairs(igpu_plan* P, const std::vector<std::pair<int, int>>& pairs, std::vector<double>& q,
+                        std::vector<unsigned char>& done) {
+  q.assign(pairs.size(), 0.0);
+  done.assign(pairs.size(), 0);
+  const int nsh = (int)P->sshells.size();
+  std::map<std::pair<int, int>, std::vector<int>> by_class;
+  for (size_t x = 0; x < pairs.size(); ++x) {
+    const SchwarzShell& a = P->sshells[pairs[x].first];
+    const SchwarzShell& b = P->sshells[pairs[x].second];
+    const long long np = (long long)a.exps.size() * (long long)b.exps.size();
+    if (auto_picks_os(a.l + b.l, a.l + b.l, np * np)) by_class[{a.l, b.l}].push_back((int)x);
+  }
+  if (by_class.empty()) return IGPU_OK;
+  cudaStream_t s = P->stream;
+  // shell data and the Boys table
+  std::vector<double> centers(3 * (size_t)nsh), exps, coefs;
+  std::vector<int> nprim(nsh), prim_off(nsh), c2s_off(nsh, -1);
+  for (int k = 0; k < nsh; ++k) {
+    const SchwarzShell& sh = P->sshells[k];
+    for (int c = 0; c < 3; ++c) centers[3 * k + c] = sh.center[c];
+    nprim[k] = (int)sh.exps.size();
+    prim_off[k] = (int)exps.size();
+    exps.insert(exps.end(), sh.exps.begin(), sh.exps.end());
+    coefs.insert(coefs.end(), sh.coefs.begin(), sh.coefs.end());
+    if (sh.c2s) c2s_off[k] = (int)(sh.c2s - P->c2s.data());
+  }
+  DevBuf<double> d_centers, d_exps, d_coefs, d_boys, d_kappa, d_q, d_scratch;
+  DevBuf<int> d_nprim, d_prim_off, d_c2s_off, d_pi, d_pj, d_eoff;
+  DevBuf<long long> d_kappa_off;
+  CK(d_centers.upload(centers, s));
+  CK(d_exps.upload(exps, s));
+  CK(d_coefs.upload(coefs, s));
+  CK(d_nprim.upload(nprim, s));
+  CK(d_prim_off.upload(prim_off, s));
+  CK(d_c2s_off.upload(c2s_off, s));
+  CK(d_boys.upload(schwarz_boys_table(), s));
+  sc::BoysDev B = schwarz_boys_view();
+  B.tab = d_boys.p;
+  const size_t budget = (size_t)2 << 30;  // scratch bytes per class launch
+  for (const auto& kv : by_class) {
+    const std::vector<int>& xs = kv.second;
+    std::vector<int> pi(xs.size()), pj(xs.size());
+    std::vector<long long> koff(xs.size());
+    std::vector<double> kap;
+    int maxpp = 1;
+    for (size_t t = 0; t < xs.size(); ++t) {
+      const SchwarzShell& a = P->sshells[pairs[xs[t]].first];
+      const SchwarzShell& b = P->sshells[pairs[xs[t]].second];
+      pi[t] = pairs[xs[t]].first;
+      pj[t] = pairs[xs[t]].second;
+      koff[t] = (long long)kap.size();
+      kap.resize(kap.size() + a.exps.size() * b.exps.size());
+      schwarz_kappa(a, b, kap.data() + koff[t]);
+      maxpp = std::max(maxpp, (int)(a.exps.size() * b.exps.size()));
+    }
+    std::vector<int> eoff;
+    sc::SClass C = schwarz_class_layout(kv.first.first, kv.first.second, maxpp, eoff);
+    CK(d_eoff.upload(eoff, s));
+    C.eoff = d_eoff.p;
+    const size_t per_block = (size_t)128 * C.total * sizeof(double);
+    const size_t want = (xs.size() + 127) / 128;
+    const int grid = (int)std::max<size_t>(1, std::min(want, std::max<size_t>(1, budget / per_block)));
+    CK(d_scratch.ensure((size_t)grid * 128 * C.total));
+    CK(d_pi.upload(pi, s));
+    CK(d_pj.upload(pj, s));
+    CK(d_kappa_off.upload(koff, s));
+    CK(d_kappa.upload(kap, s));
+    CK(d_q.ensure(xs.size()));
+    SchwarzPairsDev in{(int)xs.size(), d_pi.p, d_pj.p, d_centers.p, d_nprim.p, d_prim_off.p, d_exps.p, d_coefs.p,
+                       d_c2s_off.p, P->d_c2s.p, d_kappa_off.p, d_kappa.p};
+    CK(launch_schwarz_exact(B, C, in, d_scratch.p, grid, d_q.p, s));
+    std::vector<double> hq(xs.size());
+    CK(cudaMemcpyAsync(hq.data(), d_q.p, hq.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    // the host vectors above are read by queued copies: finish this class
+    CK(cudaStreamSynchronize(s));
+    for (size_t t = 0; t < xs.size(); ++t) {
+      q[xs[t]] = hq[t];
+      done[xs[t]] = 1;
+    }
+  }
+  return IGPU_OK;
+}
+
+// Replace the device (P|P) Q of every canonical pair for which the
+// reference's Auto policy picks OS/HGP by its bit-exact evaluation in the
 // reference orientation (shell i, shell j), so that every threshold
 // comparison of the screening is the reference's.
-void exact_schwarz(igpu_plan* P) {
+int exact_schwarz(igpu_plan* P) {
   std::vector<std::pair<int, int>> ij(P->npairs);
   for (int p = 0; p < P->npairs; ++p) ij[p] = {P->pairs[p].i, P->pairs[p].j};
   std::vector<double> q;
   std::vector<unsigned char> done;
-  schwarz_exact_many(P->sshells, ij, q, done, 0);
+  const int rc = exact_schwarz_pairs(P, ij, q, done);
+  if (rc) return rc;
   P->schwarz_exact_pairs = 0;
   for (int p = 0; p < P->npairs; ++p) {
     if (!done[p]) continue;
@@ -521,6 +659,23 @@ void exact_schwarz(igpu_plan* P) {
     P->schwarz[(size_t)i * P->nsh + j] = q[p];
     P->schwarz[(size_t)j * P->nsh + i] = q[p];
   }
+  return IGPU_OK;
+}
+
+// The primitive pairs and their FP32 copy to the device.
+cudaError_t upload_prims(igpu_plan* P) {
+  std::vector<PrimPairF> f(P->prims.size());
+  for (size_t k = 0; k < f.size(); ++k) {
+    const PrimPairD& d = P->prims[k];
+    f[k] = PrimPairF{(float)d.zeta, (float)d.e, (float)d.pax, (float)d.pay, (float)d.paz,
+                     (float)d.alpha, (float)d.beta, 0.f};
+  }
+  cudaError_t e = P->d_prims.upload(P->prims, P->stream);
+  if (e != cudaSuccess) return e;
+  e = P->d_primsf.upload(f, P->stream);
+  if (e != cudaSuccess) return e;
+  // the host copy goes out of scope: finish the transfer
+  return cudaStreamSynchronize(P->stream);
 }
 
 // One launch whose ket list is owned by the launch: bra b runs kets
@@ -683,7 +838,7 @@ int igpu_plan_create(const igpu_shell* sh, size_t nsh, int engine, igpu_plan** o
   CK(cudaEventCreate(&P->ev1));
   CK(P->d_shells.upload(P->shells, P->stream));
   CK(P->d_pairs.upload(P->pairs, P->stream));
-  CK(P->d_prims.upload(P->prims, P->stream));
+  CK(upload_prims(P.get()));
   CK(P->d_c2s.upload(P->c2s, P->stream));
   CK(P->d_counters.ensure(1));
   // class lists (device) in pair order for the Schwarz pass
@@ -698,7 +853,8 @@ int igpu_plan_create(const igpu_shell* sh, size_t nsh, int engine, igpu_plan** o
   }
   rc = run_schwarz(P.get());
   if (rc) return rc;
-  exact_schwarz(P.get());
+  rc = exact_schwarz(P.get());
+  if (rc) return rc;
   // re-sort every class by (primitive-pair count desc, Q desc, index) and
   // record the equal-count groups used to cut task segments
   {
@@ -775,7 +931,8 @@ int igpu_schwarz(const igpu_plan* Pc, double* q) {
       if (P->pairs[p].i != P->pairs[p].j) ji.push_back({P->pairs[p].j, P->pairs[p].i});
     std::vector<double> v;
     std::vector<unsigned char> done;
-    schwarz_exact_many(P->sshells, ji, v, done, 0);
+    const int rc = exact_schwarz_pairs(P, ji, v, done);
+    if (rc) return rc;
     for (size_t x = 0; x < ji.size(); ++x)
       if (done[x]) P->schwarz[(size_t)ji[x].first * P->nsh + ji[x].second] = v[x];
     P->schwarz_upper_done = true;

@@ -119,7 +119,7 @@ int igpu_plan_attach_aux(igpu_plan* P, const igpu_shell* aux, size_t naux_sh) {
   P->naux = acc;
   CK(P->d_shells.upload(P->shells, P->stream));
   CK(P->d_pairs.upload(P->pairs, P->stream));
-  CK(P->d_prims.upload(P->prims, P->stream));
+  CK(upload_prims(P));
   // aux Schwarz factors (Basis::schwarz_aux_bounds, src/df.rs:250-286): one
   // (P s|P s) quartet per aux shell, Coulomb operator
   {

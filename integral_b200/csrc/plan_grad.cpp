@@ -169,18 +169,9 @@ int igpu_autotune_grad(igpu_plan* P, const igpu_term* coulomb, int ncoul, const 
                        double threshold, int precision) {
   if (!P) return fail(IGPU_ERR_INVALID_ARGUMENT, "NULL argument");
   std::vector<double> out((size_t)P->natom * 3);
-  const int cand[] = {4, 8, 16, 32, 64};
-  std::map<int, std::map<int, float>> best;  // class key -> chunk -> shortest time
-  for (int rep = 0; rep < 2; ++rep)
-    for (int m : cand) {
-      P->tune_mult = m;
-      int rc = igpu_grad(P, coulomb, ncoul, exchange, nexch, nullptr, 0, threshold, precision, out.data());
-      P->tune_mult = 0;
-      if (rc) return rc;
-      tune_record(P, m, true, best);
-    }
-  tune_keep(P, best);
-  return IGPU_OK;
+  return tune_two_stage(P, true, [&] {
+    return igpu_grad(P, coulomb, ncoul, exchange, nexch, nullptr, 0, threshold, precision, out.data());
+  });
 }
 
 }  // extern "C"

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <map>
 #include <memory>
@@ -24,6 +25,7 @@
 #include "host_schwarz.hpp"
 #include "launch.hpp"
 #include "noalloc.hpp"
+#include "schwarz_dev.hpp"
 
 namespace igpu {
 namespace host {
@@ -147,6 +149,7 @@ struct igpu_plan {
   DevBuf<DevShell> d_shells;
   DevBuf<PairD> d_pairs;
   DevBuf<PrimPairD> d_prims;
+  DevBuf<PrimPairF> d_primsf;  // FP32 copy for the FP32 launches
   DevBuf<double> d_c2s;
   DevBuf<int> d_class_lists;
   std::vector<int> class_list_off;
@@ -166,6 +169,11 @@ struct igpu_plan {
   // overrides every launch while the tuner measures
   std::map<int, int> tuned_mult;
   int tune_mult = 0;
+  // blocks-per-SM cap of the grid per launch class (0: the occupancy limit);
+  // tune_bps != 0 overrides every launch while the tuner measures (-1: the
+  // occupancy limit)
+  std::map<int, int> tuned_bps;
+  int tune_bps = 0;
   std::unique_ptr<TaskSet> dense_tasks;
   double mixed_cutoff = 1e-4;
   // primitive screen of the FP32 launches of the mixed path: bound * max|D|
@@ -199,7 +207,7 @@ namespace host {
 
 // plan.cpp: the core every entry point shares
 int ensure_constants(int dev);
-size_t grid_for(const KernelEntry* e, bool fp32, unsigned long long total);
+size_t grid_for(const KernelEntry* e, bool fp32, unsigned long long total, int bps_cap = 0);
 KernelArgs base_args(igpu_plan* P);
 double model_flops_prim(int la, int lb, int lc, int ld);
 double model_flops_quartet(int la, int lb, int lc, int ld, bool sph, int ndens, bool jk);
@@ -208,7 +216,8 @@ double model_flops_grad_quartet(int la, int lb, int lc, int ld, bool sph, int nt
 double mixed_split(double cutoff, double dmax);
 int tune_key(int pcb, int pck, bool fp32, bool grad);
 void tune_record(igpu_plan* P, int m, bool grad, std::map<int, std::map<int, float>>& best);
-void tune_keep(igpu_plan* P, const std::map<int, std::map<int, float>>& best);
+void tune_keep(igpu_plan* P, const std::map<int, std::map<int, float>>& best, bool bps);
+int tune_two_stage(igpu_plan* P, bool grad, const std::function<int()>& run);
 size_t slot_with_acc(const KernelEntry* e, int pcb, const KernelArgs& A);
 int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t& launches);
 int collect_profile(igpu_plan* P, int ndens, bool jk, int grad_terms_c = -1, int grad_terms_x = 0);
@@ -222,7 +231,10 @@ TaskSet* cached_tasks(igpu_plan* P, double threshold, double fp64_cut, int& rc);
 int check_bra_subset(igpu_plan* P, const uint32_t* sub, size_t nsub, std::vector<unsigned>& bitmap,
                      bool accumulate);
 int run_schwarz(igpu_plan* P);
-void exact_schwarz(igpu_plan* P);
+cudaError_t upload_prims(igpu_plan* P);
+int exact_schwarz(igpu_plan* P);
+int exact_schwarz_pairs(igpu_plan* P, const std::vector<std::pair<int, int>>& pairs, std::vector<double>& q,
+                        std::vector<unsigned char>& done);
 
 }  // namespace host
 }  // namespace igpu

@@ -104,18 +104,9 @@ int igpu_autotune_jk(igpu_plan* P, const double* d_dens, int ndens, double thres
   DevBuf<double> tj, tk;
   CK(tj.ensure(n2));
   CK(tk.ensure(n2));
-  const int cand[] = {4, 8, 16, 32, 64};
-  std::map<int, std::map<int, float>> best;  // class key -> chunk -> shortest time
-  for (int rep = 0; rep < 2; ++rep)
-    for (int m : cand) {
-      P->tune_mult = m;
-      int rc = igpu_jk_device(P, d_dens, ndens, nullptr, 0, threshold, 1, precision, tj.p, tk.p, stream);
-      P->tune_mult = 0;
-      if (rc) return rc;
-      tune_record(P, m, false, best);
-    }
-  tune_keep(P, best);
-  return IGPU_OK;
+  return tune_two_stage(P, false, [&] {
+    return igpu_jk_device(P, d_dens, ndens, nullptr, 0, threshold, 1, precision, tj.p, tk.p, stream);
+  });
 }
 
 int igpu_jk(igpu_plan* P, const double* dens, int ndens, const uint32_t* bra_subset, size_t nsub, double threshold,

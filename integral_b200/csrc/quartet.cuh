@@ -88,9 +88,8 @@ struct TeamShape {
 // the Coulomb prefactor 2 pi^{5/2} / (p q sqrt(p + q)) (every Rys weight sum
 // and Boys value is <= 1); evaluated in FP32 for the primitive screen of the
 // FP32 launches.
-__device__ __forceinline__ float prim_bound(const PrimPairD& b, const PrimPairD& k) {
-  const float p = (float)b.zeta, q = (float)k.zeta;
-  return fabsf((float)b.e * (float)k.e) * (34.98683665f / (p * q * sqrtf(p + q)));
+__device__ __forceinline__ float prim_bound(const PrimPairF& b, const PrimPairF& k) {
+  return fabsf(b.e * k.e) * (34.98683665f / (b.zeta * k.zeta * sqrtf(b.zeta + k.zeta)));
 }
 
 // Largest primitive-quartet count the team screen compacts (16 x 16 primitive
@@ -107,19 +106,31 @@ __device__ __forceinline__ void accumulate_thread(const KernelArgs& A, const R* 
 #pragma unroll
   for (int q = 0; q < S::NG; ++q) G[q] = R(0);
   const float cut = (sizeof(R) == 4 && A.fp32) ? (float)A.prim_cut : 0.f;
+  float acx = 0.f, acy = 0.f, acz = 0.f;
+  if constexpr (sizeof(R) == 4) {
+    const DevShell& sa = A.shells[pb.a];
+    const DevShell& sc = A.shells[pk.a];
+    acx = (float)(sa.cx - sc.cx);
+    acy = (float)(sa.cy - sc.cy);
+    acz = (float)(sa.cz - sc.cz);
+  }
   for (int ip = 0; ip < pb.nprim; ++ip) {
-    const PrimPairD bp = A.prims[pb.prim_off + ip];
     for (int kq = 0; kq < pk.nprim; ++kq) {
-      const PrimPairD kp = A.prims[pk.prim_off + kq];
-      if constexpr (sizeof(R) == 4)
+      QuartetHdr<R> h;
+      if constexpr (sizeof(R) == 4) {
+        const PrimPairF bp = A.primsf[pb.prim_off + ip];
+        const PrimPairF kp = A.primsf[pk.prim_off + kq];
         if (cut > 0.f && prim_bound(bp, kp) < cut) continue;
-      const QuartetHdr<R> h = quartet_header<R>(bp, kp, A.omega);
+        h = quartet_header_f(bp, kp, acx, acy, acz, A.omega);
+      } else {
+        h = quartet_header<R>(A.prims[pb.prim_off + ip], A.prims[pk.prim_off + kq], A.omega);
+      }
       R x[NR], w[NR];
       if constexpr (sizeof(R) == 4) {
         // FP32 launch: high l and T just below the asymptotic crossover take
         // FP64 roots and weights
         if (roots_in_fp64<NR, R>(h.T)) {
-          const double T64 = quartet_T64(bp, kp, A.omega);
+          const double T64 = quartet_T64(A.prims[pb.prim_off + ip], A.prims[pk.prim_off + kq], A.omega);
 #pragma unroll
           for (int r = 0; r < NR; ++r) {
             double xd, wd;
@@ -222,6 +233,14 @@ __device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, c
   const int npk = pk.nprim;
   const int myp = lane % BP;
   const int sub = lane / BP;
+  float acx = 0.f, acy = 0.f, acz = 0.f;
+  if constexpr (sizeof(R) == 4) {
+    const DevShell& sa = A.shells[pb.a];
+    const DevShell& sc = A.shells[pk.a];
+    acx = (float)(sa.cx - sc.cx);
+    acy = (float)(sa.cy - sc.cy);
+    acz = (float)(sa.cz - sc.cz);
+  }
   for (int base = 0; base < npr; base += BP) {
     const int nb = npr - base < BP ? npr - base : BP;
     const bool active = myp < nb;
@@ -230,13 +249,14 @@ __device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, c
     if (active) {
       const int pidx = surv ? (int)surv[base + myp] : base + myp;
       const int ip = pidx / npk, kq = pidx - ip * npk;
-      const PrimPairD& bpp = A.prims[pb.prim_off + ip];
-      const PrimPairD& kpp = A.prims[pk.prim_off + kq];
-      h = quartet_header<R>(bpp, kpp, A.omega);
+      if constexpr (sizeof(R) == 4)
+        h = quartet_header_f(A.primsf[pb.prim_off + ip], A.primsf[pk.prim_off + kq], acx, acy, acz, A.omega);
+      else
+        h = quartet_header<R>(A.prims[pb.prim_off + ip], A.prims[pk.prim_off + kq], A.omega);
       // FP32 launch: high l and T just below the asymptotic crossover take
       // FP64 roots and weights
       const bool r64 = roots_in_fp64<NR, R>(h.T);
-      const double T64 = r64 ? quartet_T64(bpp, kpp, A.omega) : 0.0;
+      const double T64 = r64 ? quartet_T64(A.prims[pb.prim_off + ip], A.prims[pk.prim_off + kq], A.omega) : 0.0;
       for (int r = sub; r < NR; r += SUB) {
         R xr, wr;
         if (r64) {
@@ -339,7 +359,7 @@ __device__ __forceinline__ int screen_prims(const KernelArgs& A, const PairD& pb
     bool keep = false;
     if (pidx < npr) {
       const int ip = pidx / npk, kq = pidx - ip * npk;
-      keep = prim_bound(A.prims[pb.prim_off + ip], A.prims[pk.prim_off + kq]) >= cut;
+      keep = prim_bound(A.primsf[pb.prim_off + ip], A.primsf[pk.prim_off + kq]) >= cut;
     }
     const unsigned bal = (__ballot_sync(tmask, keep) & tmask) >> shift;
     if (keep) list[n + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)pidx;

@@ -23,7 +23,9 @@ def parse(src, name):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        raise SystemExit("usage: extract_rys_tables.py <reference root> [<output .inc>]")
+    root = sys.argv[1]
     here = os.path.dirname(os.path.abspath(__file__))
     out = sys.argv[2] if len(sys.argv) > 2 else os.path.join(here, "_ref", "rys_tables.inc")
     path = os.path.join(root, "crates", "integral", "src", "math", "rys_tables.rs")

@@ -56,7 +56,9 @@ def parse_rys(root):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        raise SystemExit("usage: make_golden.py <reference root>")
+    root = sys.argv[1]
     with open(os.path.join(HERE, "c2s_signed.json"), "w") as f:
         json.dump({"source": "crates/integral/tests/c2s_independent_reference.rs (C2S_SIGNED_REF)",
                    "rows": parse_c2s(root)}, f, indent=1)

@@ -1,8 +1,8 @@
 """GPU parity of the g-shell classes (l = 4, the highest shell of the
 molecule-batch workload) against the oracle: the dense tensor and single
-(gg|gg) blocks, Cartesian and spherical, within the dense-ERI contract, and
-direct J/K with the exact screened quartet list; the gradient of a basis
-with g shells is reported unsupported (its classes are not compiled)."""
+(gg|gg) blocks, Cartesian and spherical, within the reference's contract
+between its own engines, direct J/K with the exact screened quartet list,
+and the gradient (raised tables to l = 5)."""
 import numpy as np
 import pytest
 
@@ -14,11 +14,13 @@ pytestmark = pytest.mark.gpu
 
 
 def check_eri(gpu, ref):
-    peak = float(np.max(np.abs(ref)))
+    """The reference's own contract between its two engines,
+    |os - rys| <= 1e-11 + 1e-10 |x| element-wise (tests/cross_engine.rs:40-56):
+    the GPU's quadrature against the Auto (OS/HGP) evaluation.  On g blocks of
+    two-primitive shells the reference's own OS and Rys engines differ by up
+    to 7e-9 relative on significant elements (3e-11 of the peak)."""
     d = np.abs(gpu - ref)
-    sig = np.abs(ref) >= 1e-3 * peak
-    assert float(np.max(d[sig] / np.abs(ref[sig]))) < 1e-12
-    assert float(np.max(d)) < 1e-13 * max(peak, 1.0)
+    assert np.all(d <= 1e-11 + 1e-10 * np.abs(ref)), float(np.max(d - 1e-10 * np.abs(ref)))
 
 
 def two_centre_g(spherical):
@@ -71,14 +73,18 @@ def test_jk_with_g_shells_exact_list():
     assert abs(e(Jm, Km) - e(J, K)) < 1e-7
 
 
-def test_gradient_of_g_shells_is_reported_unsupported():
-    """The gradient classes stop at f (their raised tables reach l = 4); a
-    basis with g shells gets IGPU_ERR_UNSUPPORTED, never a wrong result."""
-    shells, D = molecule(2, 8)
+def test_gradient_with_g_shells():
+    """The gradient classes of g shells (raised tables to l = 5): the exact
+    screened list, and the gradient within 1e-10 of its maximum against the
+    oracle (whose shifted classes the Auto policy also sends to OS/HGP)."""
+    shells, D = molecule(3, 8)
     gc = ib.Basis(shells).direct_grad_contractor()
-    dens = gc.density([ib.GradDensityTerm(0.5, D[0], D[0])], [ib.GradDensityTerm(-0.25, D[0], D[0])])
+    coul, exch = [(0.5, D[0], D[0])], [(-0.25, D[0], D[0])]
+    dens = gc.density([ib.GradDensityTerm(*t) for t in coul], [ib.GradDensityTerm(*t) for t in exch])
     out = np.zeros((gc.natom(), 3))
-    with pytest.raises(ib.IntegralError) as e:
-        gc.accumulate_bra_pairs(ib.DirectGradWorkspace(), None, dens, 1e-11, out)
-    assert e.value.code == -11 and "gradient classes" in str(e.value)
-    assert np.all(out == 0.0)
+    gc.accumulate_bra_pairs(ib.DirectGradWorkspace(), None, dens, 1e-11, out)
+    st = gc.last_stats()
+    ref, cnt, hsh = O.OracleBasis(shells).direct_grad(coul, exch, 1e-11, nthreads=16)
+    assert st["quartets"] == cnt and st["quartet_hash"] == hsh
+    assert float(np.max(np.abs(out - ref))) < 1e-10 * float(np.max(np.abs(ref)))
+    assert float(np.max(np.abs(out.sum(axis=0)))) < 1e-9 * float(np.max(np.abs(out)))

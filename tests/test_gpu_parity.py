@@ -40,6 +40,12 @@ def energy(D, J, K):
     return sum(0.5 * float(np.sum(D[d] * (J[d] - 0.5 * K[d]))) for d in range(len(D)))
 
 
+def test_oracle_checks_with_the_reference_rys_tables():
+    """The oracle that checks the GPU here carries the reference's literal
+    Rys coefficients (extracted at its build), not its own regeneration."""
+    assert O.lib().orc_rys_tables_are_reference_literals()
+
+
 def test_product_library_is_the_one_loaded():
     s = S.dense_eri_system()
     ib.Basis(s["shells"]).plan()
