@@ -401,6 +401,7 @@ def batch_bench(args):
     nmol = len(mols)
     steps = args.steps
     h2d = int(8 * sum(D.size for D in dens))
+    natoms = int(sum(batch.natom(m) for m in range(nmol)))
     # CPU baseline: the oracle's J/K on every host thread over seeded bra
     # samples of a seeded sample of molecules; its screened quartets per
     # second over the batch's mean quartets per molecule give molecules/s
@@ -430,14 +431,14 @@ def batch_bench(args):
         "config": {"workload": "256 molecules, 4..40 atoms, s,s,p,p,d,f,g spherical, 3 primitives, one density "
                                "each (nocc = nao/4), tau 1e-11, one CUDA graph per step%s"
                                % ("" if want_grad else "; J/K only (gradient classes of g shells not compiled)"),
-                   "molecules": nmol, "atoms": int(sum(batch.natom(m) for m in range(nmol))),
+                   "molecules": nmol, "atoms": natoms,
                    "nao_total": int(sum(batch.nao(m) for m in range(nmol))), "quartets_per_step": q32 // steps,
                    "batch_setup_s": setup_s, "l2": "flushed between steps (512 MB write)"},
         "fp64": {"value": nmol * steps / (ms64 * 1e-3), "unit": "molecules/s", "ms_per_step": ms64 / steps,
                  "mixed_speedup": ms64 / ms32},
         "energy_error_mixed_vs_fp64_Eh": {"max_abs": float(np.max(np.abs(dE))), "sum": float(np.sum(dE))},
         "e2e": {"value": nmol * steps / w32, "unit": "molecules/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": 2 * h2d},
+                "d2h_bytes_per_step": 2 * h2d + (24 * natoms if want_grad else 0)},
         "clocks": clocks,
         "gpu_launches": l32,
         "cpu_baseline": {"value": cpu_q / cpu_s / q_per_mol, "unit": "molecules/s", "cores": nthreads,

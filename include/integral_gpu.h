@@ -133,9 +133,11 @@ int igpu_atoms(const igpu_plan* plan, double* xyz);
 /* Basis::schwarz_bounds (integrals.rs:835-862): nsh x nsh, row-major.
  * Wherever the reference's Auto policy (integrals.rs:374-388) evaluates a
  * diagonal quartet with OS/HGP, which covers every shell pair of a basis of
- * contracted shells, the plan holds the host's bit-exact evaluation of it,
- * so the screened quartet lists equal the reference's by construction; the
- * other pairs (see igpu_schwarz_bounds) keep the device's Rys evaluation. */
+ * contracted shells, the plan holds a bit-exact evaluation of it (run on the
+ * device with the reference's order of operations and no fused
+ * multiply-adds), so the screened quartet lists equal the reference's by
+ * construction; the other pairs (see igpu_schwarz_bounds) keep the device's
+ * Rys evaluation.  Molecule batches hold the same bounds. */
 int igpu_schwarz(const igpu_plan* plan, double* q);
 /* Basis::schwarz_bounds of a shell list on the host, without a device or a
  * plan: the same bit-exact bounds, nsh x nsh row-major.  An ordered shell

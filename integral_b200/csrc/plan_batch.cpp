@@ -162,6 +162,7 @@ int igpu_batch_create(const igpu_shell* sh, const size_t* mol_nsh, size_t nmol, 
   // shells at m*S + local (padding entries have no functions and no pairs),
   // atoms by bitwise-equal centre inside each molecule (src/shell.rs:250-258)
   P->shells.assign((size_t)b->S * nmol, DevShell{});
+  P->sshells.assign((size_t)b->S * nmol, SchwarzShell{});
   std::vector<double> expv, eff;
   int lmax = 0;
   s0 = 0;
@@ -199,6 +200,13 @@ int igpu_batch_create(const igpu_shell* sh, const size_t* mol_nsh, size_t nmol, 
       lmax = std::max(lmax, d.l);
       const size_t g = m * b->S + q;
       P->shells[g] = d;
+      SchwarzShell& ss = P->sshells[g];
+      ss.l = d.l;
+      ss.center[0] = d.cx;
+      ss.center[1] = d.cy;
+      ss.center[2] = d.cz;
+      ss.exps.assign(expv.end() - d.nprim, expv.end());
+      ss.coefs.assign(eff.end() - d.nprim, eff.end());
     }
     b->mol_natom.push_back((int)(P->atoms.size() - a0));
     s0 += mol_nsh[m];
@@ -215,6 +223,8 @@ int igpu_batch_create(const igpu_shell* sh, const size_t* mol_nsh, size_t nmol, 
     P->c2s.insert(P->c2s.end(), mm.begin(), mm.end());
   }
   P->c2s_off[GPU_MAX_L + 2] = (int)P->c2s.size();
+  for (size_t g = 0; g < P->shells.size(); ++g)
+    if (P->shells[g].nfunc && P->shells[g].spherical) P->sshells[g].c2s = P->c2s.data() + P->c2s_off[P->shells[g].l];
   // canonical pairs inside each molecule (integrals.rs:1252-1260, local
   // order) with their primitive pairs in evaluation orientation
   // (os_eri.rs:211-244); tri is the local canonical index, which orders the
@@ -285,11 +295,9 @@ int igpu_batch_create(const igpu_shell* sh, const size_t* mol_nsh, size_t nmol, 
     }
     CK(P->d_class_lists.upload(flat, P->stream));
   }
-  // The batch screens with the device's (P|P) Schwarz bounds (within 1e-14
-  // of the reference's): the host's bit-exact evaluation of every diagonal
-  // quartet of hundreds of molecules with g shells would take tens of
-  // minutes of host time at batch creation.
   rc = run_schwarz(P);
+  if (rc) return rc;
+  rc = exact_schwarz(P);
   if (rc) return rc;
   // every class sorted by (molecule, primitive-pair count desc, Q desc);
   // groups are the runs of equal (molecule, count), indexed per molecule

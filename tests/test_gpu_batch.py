@@ -61,11 +61,10 @@ def test_batch_equals_per_molecule_plans(letters):
         assert rel(Jb, Jm) < 1e-12 and rel(Kb, Km) < 1e-12
         if gradient:
             assert rel(Gb, Gm) < 1e-12
-    # every quartet of every molecule: the batch screens with the device's
-    # Schwarz bounds (within 1e-14 of the reference's, which the single
-    # plans use), so only quartets at the threshold itself may differ
+    # every quartet of every molecule, and no other: the batch screens with
+    # the same bit-exact Schwarz bounds as the single plans
     batch.jk_grad([m[1] for m in mols], thr, gradient=False)
-    assert abs(batch.last_stats()["quartets"] - total) <= 1e-6 * total + 8
+    assert batch.last_stats()["quartets"] == total
     # two molecules against the oracle
     for k in (1, 4):
         shells, D = mols[k]
