@@ -75,6 +75,8 @@ def parse():
     # a stride > 1 still decodes every task (the subset is a filter), so its
     # quartets/s understates the full build's
     p.add_argument("--grad-stride", type=int, default=1)
+    p.add_argument("--mixed-cutoff", type=float, default=None,
+                   help="Schwarz-product cutoff below which quartets run in FP32 (default: the library's)")
     p.add_argument("--profile-case", action="store_true",
                    help="one FP32-mixed J/K build of the 24-atom (nao 360) system and its per-launch "
                         "records, no timing: the small case for ncu captures")
@@ -97,6 +99,8 @@ def grad_bench(args):
 
     s = S.grad_system()
     gc = ib.Basis(s["shells"]).direct_grad_contractor()
+    if args.mixed_cutoff is not None:
+        gc.set_mixed_cutoff(args.mixed_cutoff)
     dens = gc.density([ib.GradDensityTerm(f, l, r) for f, l, r in s["coulomb"]],
                       [ib.GradDensityTerm(f, l, r) for f, l, r in s["exchange"]])
     bras = np.arange(0, len(gc.bra_pairs()), args.grad_stride)
@@ -281,7 +285,11 @@ def jk_sph_bench(args):
     system = S.jk_spherical_system()
     nd = system["dens"].shape[0]
     thr = system["threshold"]
+    t0 = time.perf_counter()
     dc = ib.Basis(system["shells"]).direct_contractor()
+    plan_s = time.perf_counter() - t0
+    if args.mixed_cutoff is not None:
+        dc.set_mixed_cutoff(args.mixed_cutoff)
     nbra = len(dc.bra_pairs())
     bras = np.arange(0, nbra, args.sph_stride, dtype=np.uint32)
     D = torch.from_numpy(system["dens"]).cuda()
@@ -310,13 +318,17 @@ def jk_sph_bench(args):
             ms += e0.elapsed_time(e1)
             st = dc.last_stats()
             q += st["quartets"]
-            launches += st["launches"] + 4
+            share[0] = st["quartets_fp32"] / max(st["quartets"], 1)
+            launches += st["launches"] + 5
         return ms, q, launches
+
+    share = [0.0]
 
     clk = ClockSampler(0)
     clk.start()
     ms32, q32, l32 = timed(1, args.warmup, args.steps)
     clocks = clk.stop()
+    fp32_share = share[0]
     Jm, Km = J.cpu().numpy().copy(), K.cpu().numpy().copy()
     ms64, q64, _ = timed(0, 1, args.steps)
     J64, K64 = J.cpu().numpy(), K.cpu().numpy()
@@ -331,7 +343,9 @@ def jk_sph_bench(args):
         "config": {"workload": "direct J/K, 200 atoms in 32-bohr cube, s,s,s,p,p,d,d,f spherical, 4 primitives, "
                                "nao 5200, 2 densities, tau 1e-11, every %d-th canonical bra pair (%d of %d)"
                                % (args.sph_stride, len(bras), nbra),
-                   "quartets_per_step": q32 // st, "l2": "flushed between steps (512 MB write)"},
+                   "quartets_per_step": q32 // st, "l2": "flushed between steps (512 MB write)",
+                   "plan_s": plan_s, "mixed_cutoff": dc.mixed_cutoffs()[0], "mixed_prim_eps": dc.mixed_cutoffs()[1],
+                   "fp32_quartet_share": fp32_share},
         "fp64": {"value": q64 / (ms64 * 1e-3), "unit": "quartets/s", "ms_per_step": ms64 / st,
                  "mixed_speedup": ms64 / ms32},
         "energy_error_mixed_vs_fp64_Eh_on_sample": dE,
@@ -365,6 +379,8 @@ def batch_bench(args):
     t0 = time.perf_counter()
     batch = ib.MoleculeBatch([m["shells"] for m in mols])
     setup_s = time.perf_counter() - t0
+    if args.mixed_cutoff is not None:
+        batch.set_mixed_cutoff(args.mixed_cutoff)
     dens = [m["dens"] for m in mols]
     want_grad = False
     try:
@@ -395,6 +411,7 @@ def batch_bench(args):
     clk.start()
     ms32, w32, q32, l32, out32, st32 = timed(1)
     clocks = clk.stop()
+    fp32_share = st32["quartets_fp32"] / max(st32["quartets"], 1)
     ms64, w64, q64, _, out64, _ = timed(0)
     dE = [0.5 * float(np.sum(D * ((a - c) - 0.5 * (b - d))))
           for D, a, b, c, d in zip(dens, out32[0], out32[1], out64[0], out64[1])]
@@ -433,7 +450,9 @@ def batch_bench(args):
                                % ("" if want_grad else "; J/K only (gradient classes of g shells not compiled)"),
                    "molecules": nmol, "atoms": natoms,
                    "nao_total": int(sum(batch.nao(m) for m in range(nmol))), "quartets_per_step": q32 // steps,
-                   "batch_setup_s": setup_s, "l2": "flushed between steps (512 MB write)"},
+                   "batch_setup_s": setup_s, "l2": "flushed between steps (512 MB write)",
+                   "mixed_cutoff": args.mixed_cutoff if args.mixed_cutoff is not None else "library default",
+                   "fp32_quartet_share": fp32_share},
         "fp64": {"value": nmol * steps / (ms64 * 1e-3), "unit": "molecules/s", "ms_per_step": ms64 / steps,
                  "mixed_speedup": ms64 / ms32},
         "energy_error_mixed_vs_fp64_Eh": {"max_abs": float(np.max(np.abs(dE))), "sum": float(np.sum(dE))},
@@ -677,6 +696,8 @@ def main():
     thr = system["threshold"]
     basis = ib.Basis(system["shells"])
     dc = basis.direct_contractor()
+    if args.mixed_cutoff is not None:
+        dc.set_mixed_cutoff(args.mixed_cutoff)
     nbra = len(dc.bra_pairs())
     bras = None if world == 1 else sharding.bra_shard(nbra, rank, world)
 
@@ -718,7 +739,8 @@ def main():
             times.append(e0.elapsed_time(e1))
             st = dc.last_stats()
             quartets += st["quartets"]
-            launches += st["launches"] + 4  # + bounds, symmetry check, 2 symmetrisations
+            fp32q[0] = st["quartets_fp32"] / max(st["quartets"], 1)
+            launches += st["launches"] + 5  # + bounds, symmetry check, FP32 densities, 2 symmetrisations
             prof = dc.plan.profile()
         clocks = sampler.stop() if sampler else None
         t = sum(times)
@@ -732,8 +754,10 @@ def main():
             quartets = int(qq.item())
         return t, quartets, launches, prof, clocks
 
+    fp32q = [0.0]
     sampler = ClockSampler(local) if rank == 0 else None
     t_mixed, q_mixed, l_mixed, prof_mixed, clocks = timed(1, args.warmup, args.steps, sampler)
+    fp32_share = fp32q[0]
     Jm, Km = J.cpu().numpy().copy(), K.cpu().numpy().copy()
     # an SCF caller passes a new density every iteration: time the mixed call
     # (host wall, synchronous) on a perturbed density against the same call
@@ -835,6 +859,8 @@ def main():
         "config": {"workload": "direct J/K, 64 atoms in 20-bohr cube, s,s,s,p,p,d Cartesian, nao 960, "
                                "4 densities, Schwarz tau 1e-12",
                    "nao": nao, "ndens": nd, "threshold": thr, "quartets_per_step": q_mixed // steps,
+                   "mixed_cutoff": dc.mixed_cutoffs()[0], "mixed_prim_eps": dc.mixed_cutoffs()[1],
+                   "fp32_quartet_share": fp32_share,
                    "parallelism": "bra-pair shards x%d + NCCL all-reduce" % world if world > 1 else "1 GPU",
                    "l2": "flushed between steps (512 MB write)"},
         "fp64": {"value": q_64 / (t_64 * 1e-3), "unit": UNIT, "ms_per_step": t_64 / steps,

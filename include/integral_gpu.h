@@ -57,9 +57,11 @@ extern "C" {
 
 /* Arithmetic of the quartet kernels.  FP64: every quartet in double.
  * MIXED: quartets whose Schwarz estimate Q_ij*Q_kl*M is below the plan's
- * cutoff run their Rys roots, recurrences and contraction in FP32, the rest
- * in FP64; M is max|D| (or the term matrices' maximum) rounded up to a power
- * of two, so densities whose maxima share a binade share one task list.  All
+ * cutoff run in FP32 (Rys roots, recurrences, primitive contraction and, for
+ * J/K, the horizontal recurrences, spherical transform and density
+ * contraction against an FP32 copy of the densities), the rest in FP64; M is
+ * max|D| (or the term matrices' maximum) rounded up to a power of two, so
+ * densities whose maxima share a binade share one task list.  All
  * J/K/gradient accumulation is FP64. */
 #define IGPU_PRECISION_FP64 0
 #define IGPU_PRECISION_MIXED 1
@@ -156,6 +158,8 @@ int igpu_set_mixed_cutoff(igpu_plan* plan, double cutoff);
  * times max|D| is below eps is skipped (default 1e-15).  0 evaluates every
  * primitive quartet; the FP64 path never skips one. */
 int igpu_set_mixed_prim_cutoff(igpu_plan* plan, double eps);
+/* The plan's two mixed-precision cutoffs (either pointer may be NULL). */
+int igpu_get_mixed_cutoffs(const igpu_plan* plan, double* cutoff, double* prim_eps);
 /* EriKernel (src/integrals.rs:304-321) of every later call on the plan:
  * omega = 0 is Coulomb 1/r (the default); omega > 0 finite is the long-range
  * erf(omega r)/r (Basis::eri_kernel, EriBuilder::kernel, the gradient's

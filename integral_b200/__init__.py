@@ -808,6 +808,12 @@ class DirectContractor:
         (default 1e-4) run in FP32 (igpu_set_mixed_cutoff)."""
         _lib.check(_lib.lib().igpu_set_mixed_cutoff(self._plan.h, float(cutoff)))
 
+    def mixed_cutoffs(self):
+        """(cutoff, primitive eps) of MIXED precision (igpu_get_mixed_cutoffs)."""
+        c, e = ctypes.c_double(), ctypes.c_double()
+        _lib.check(_lib.lib().igpu_get_mixed_cutoffs(self._plan.h, ctypes.byref(c), ctypes.byref(e)))
+        return c.value, e.value
+
     def set_mixed_prim_cutoff(self, eps: float):
         """MIXED precision: inside the FP32 quartets, skip primitive quartets
         whose magnitude bound times max|D| is below `eps`
@@ -885,6 +891,11 @@ class DirectGradContractor:
 
     def bra_pairs(self):
         return list(self._pairs)
+
+    def set_mixed_cutoff(self, cutoff: float):
+        """MIXED precision: quartets whose Schwarz product times the term
+        matrices' maximum is below `cutoff` run in FP32 (igpu_set_mixed_cutoff)."""
+        _lib.check(_lib.lib().igpu_set_mixed_cutoff(self._plan.h, float(cutoff)))
 
     def density(self, coulomb: Sequence[GradDensityTerm], exchange: Sequence[GradDensityTerm]) -> GradDensity:
         n2 = self._plan.nao ** 2

@@ -70,6 +70,7 @@ def lib():
     L.igpu_schwarz_bounds.argtypes = [ctypes.POINTER(IgpuShell), ctypes.c_size_t, c_double_p, c_size_p]
     L.igpu_set_mixed_cutoff.argtypes = [vp, ctypes.c_double]
     L.igpu_set_mixed_prim_cutoff.argtypes = [vp, ctypes.c_double]
+    L.igpu_get_mixed_cutoffs.argtypes = [vp, c_double_p, c_double_p]
     L.igpu_set_erf_omega.argtypes = [vp, ctypes.c_double]
     L.igpu_eri_dense.argtypes = [vp, c_double_p]
     L.igpu_eri_builder_fill.argtypes = [vp, c_u32_p, ctypes.c_size_t, c_double_p]
@@ -110,7 +111,7 @@ def lib():
 
 EXPORTED = [
     "igpu_abi_version", "igpu_last_error_string", "igpu_plan_create", "igpu_plan_destroy", "igpu_plan_query",
-    "igpu_bra_pairs", "igpu_atoms", "igpu_schwarz", "igpu_schwarz_bounds", "igpu_set_mixed_cutoff", "igpu_set_mixed_prim_cutoff", "igpu_set_erf_omega",
+    "igpu_bra_pairs", "igpu_atoms", "igpu_schwarz", "igpu_schwarz_bounds", "igpu_set_mixed_cutoff", "igpu_set_mixed_prim_cutoff", "igpu_get_mixed_cutoffs", "igpu_set_erf_omega",
     "igpu_eri_dense",
     "igpu_eri_builder_fill", "igpu_eri_screened", "igpu_eri_block", "igpu_eri_packed", "igpu_plan_attach_aux", "igpu_aux_query", "igpu_schwarz_aux",
     "igpu_eri_2c", "igpu_eri_3c", "igpu_density_shell_bounds", "igpu_jk", "igpu_jk_device", "igpu_jk_device_static",

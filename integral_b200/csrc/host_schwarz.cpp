@@ -185,7 +185,7 @@ bool schwarz_exact(const SchwarzShell& si, const SchwarzShell& sj, double& q) {
   schwarz_kappa(si, sj, kap.data());
   const sc::BoysDev B = BoysTable::get().view();
   const sc::Slice W{work.data(), 1};
-  q = sc::sc_schwarz(B, C, W, si.center, sj.center, (int)si.exps.size(), (int)sj.exps.size(), si.exps.data(),
+  q = sc::sc_schwarz(B, C, W, sc::Team{0, 1}, si.center, sj.center, (int)si.exps.size(), (int)sj.exps.size(), si.exps.data(),
                      si.coefs.data(), sj.exps.data(), sj.coefs.data(), kap.data(), si.c2s, sj.c2s);
   return true;
 }

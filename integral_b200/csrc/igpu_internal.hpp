@@ -116,6 +116,7 @@ enum Mode : int {
 
 struct JKDev {
   const double* D;       // ndens x nao x nao
+  const float* Df;       // its FP32 copy, read by the FP32 launches
   const double* bounds;  // ndens x nsh x nsh  (density_shell_bounds)
   double* J;             // symmetric: one-orientation accumulators J', K'
   double* K;             //   (J = (J' + J'^T)/2 added by the finalize pass)

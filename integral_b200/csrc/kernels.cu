@@ -141,6 +141,19 @@ cudaError_t launch_symmetrize_add(const double* H, double* out, int nmat, int na
   return cudaGetLastError();
 }
 
+// out[i] = (float)in[i]: the FP32 copy of the densities read by the FP32
+// launches of the mixed J/K path.
+__global__ void to_float_kernel(const double* __restrict__ in, float* __restrict__ out, size_t n) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[t] = (float)in[t];
+}
+
+cudaError_t launch_to_float(const double* in, float* out, size_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  to_float_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in, out, n);
+  return cudaGetLastError();
+}
+
 // flag[0] += 1 for every element with M[r][c] != M[c][r] (bitwise compare).
 __global__ void asym_count_kernel(const double* __restrict__ D, int nmat, int nao, unsigned long long* flag) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;

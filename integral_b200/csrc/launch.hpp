@@ -48,6 +48,7 @@ cudaError_t launch_quartets(const KernelEntry* e, bool fp32, int grid, const Ker
 cudaError_t launch_shell_block_max(const double* D, int nmat, const DevShell* sh, int nsh, int nao,
                                    int symmetrise, double* out, cudaStream_t s);
 cudaError_t launch_symmetrize_add(const double* H, double* out, int nmat, int nao, cudaStream_t s);
+cudaError_t launch_to_float(const double* in, float* out, size_t n, cudaStream_t s);
 cudaError_t launch_asym_count(const double* D, int nmat, int nao, unsigned long long* flag, cudaStream_t s);
 // Molecule batches (plan_batch.cpp): matrices of molecule m at m*P*(P+1),
 // row stride P; shell blocks at m*S*(S+1), row stride S.

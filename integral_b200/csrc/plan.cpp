@@ -251,6 +251,8 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     if (L->total == 0) continue;
     const KernelEntry* e = entry(L->pcb, L->pck);
     if (!e) return fail(IGPU_ERR_UNSUPPORTED, "angular class not compiled for the GPU");
+    if (A.mode == MODE_JK && L->fp32 && !A.jk.Df)
+      return fail(IGPU_ERR_INVALID_ARGUMENT, "FP32 J/K launch without the FP32 densities");
     need = std::max(need, grid_for(e, L->fp32, L->total) * (128 / e->team) * slot_with_acc(e, L->pcb, A));
   }
   CK(P->d_scratch.ensure(need));
@@ -267,6 +269,9 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
   }
   lg.profile.clear();
   lg.profile_launch.clear();
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(s, &cap));
+  const bool capturing = cap == cudaStreamCaptureStatusActive;
   for (size_t li = 0; li < nl; ++li) {
     Launch* L = ts.launches[li].get();
     if (L->total == 0) continue;
@@ -301,10 +306,13 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     A.task.total = L->total;
     A.fp32 = L->fp32 ? 1 : 0;
     A.builder_swap = L->builder_swap;
-    // external records, so that a captured graph records them on replay
-    CK(cudaEventRecordWithFlags(lg.events[2 * li], s, cudaEventRecordExternal));
+    // under stream capture the records are external nodes, so that the
+    // graph records them on every replay (the flag is only valid there)
+    CK(capturing ? cudaEventRecordWithFlags(lg.events[2 * li], s, cudaEventRecordExternal)
+                 : cudaEventRecord(lg.events[2 * li], s));
     CK(launch_quartets(e, L->fp32, (int)grid, A, s));
-    CK(cudaEventRecordWithFlags(lg.events[2 * li + 1], s, cudaEventRecordExternal));
+    CK(capturing ? cudaEventRecordWithFlags(lg.events[2 * li + 1], s, cudaEventRecordExternal)
+                 : cudaEventRecord(lg.events[2 * li + 1], s));
     ++launches;
     igpu_launch_record r{};
     r.la = pc_la_host(L->pcb);
@@ -554,7 +562,7 @@ int run_schwarz(igpu_plan* P) {
 // The reference's Schwarz bounds of the listed ordered shell pairs (i, j)
 // wherever its Auto policy evaluates (ij|ij) with OS/HGP, on the device with
 // the shared bit-exact evaluation (schwarz_core.cuh): one launch per class
-// (l_i, l_j), one thread per pair.  done[x] = 1 where q[x] was set.
+// (l_i, l_j), one thread or one warp per pair.  done[x] = 1 where q[x] was set.
 int exact_schwarz_pairs(igpu_plan* P, const std::vector<std::pair<int, int>>& pairs, std::vector<double>& q,
                         std::vector<unsigned char>& done) {
   q.assign(pairs.size(), 0.0);
@@ -614,10 +622,14 @@ int exact_schwarz_pairs(igpu_plan* P, const std::vector<std::pair<int, int>>& pa
     sc::SClass C = schwarz_class_layout(kv.first.first, kv.first.second, maxpp, eoff);
     CK(d_eoff.upload(eoff, s));
     C.eoff = d_eoff.p;
-    const size_t per_block = (size_t)128 * C.total * sizeof(double);
-    const size_t want = (xs.size() + 127) / 128;
+    // classes from l_i + l_j = 4 up run a warp per pair (their recurrence
+    // levels have hundreds of elements), the smaller ones a thread per pair
+    const int team = kv.first.first + kv.first.second >= 4 ? 32 : 1;
+    const size_t per_block_pairs = 128 / team;
+    const size_t per_block = per_block_pairs * C.total * sizeof(double);
+    const size_t want = (xs.size() + per_block_pairs - 1) / per_block_pairs;
     const int grid = (int)std::max<size_t>(1, std::min(want, std::max<size_t>(1, budget / per_block)));
-    CK(d_scratch.ensure((size_t)grid * 128 * C.total));
+    CK(d_scratch.ensure((size_t)grid * per_block_pairs * C.total));
     CK(d_pi.upload(pi, s));
     CK(d_pj.upload(pj, s));
     CK(d_kappa_off.upload(koff, s));
@@ -625,7 +637,7 @@ int exact_schwarz_pairs(igpu_plan* P, const std::vector<std::pair<int, int>>& pa
     CK(d_q.ensure(xs.size()));
     SchwarzPairsDev in{(int)xs.size(), d_pi.p, d_pj.p, d_centers.p, d_nprim.p, d_prim_off.p, d_exps.p, d_coefs.p,
                        d_c2s_off.p, P->d_c2s.p, d_kappa_off.p, d_kappa.p};
-    CK(launch_schwarz_exact(B, C, in, d_scratch.p, grid, d_q.p, s));
+    CK(launch_schwarz_exact(B, C, in, d_scratch.p, grid, team, d_q.p, s));
     std::vector<double> hq(xs.size());
     CK(cudaMemcpyAsync(hq.data(), d_q.p, hq.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
     // the host vectors above are read by queued copies: finish this class
@@ -991,6 +1003,13 @@ int igpu_set_erf_omega(igpu_plan* P, double omega) {
 int igpu_set_mixed_cutoff(igpu_plan* P, double cutoff) {
   if (!P || !(cutoff >= 0.0)) return fail(IGPU_ERR_INVALID_ARGUMENT, "invalid cutoff");
   P->mixed_cutoff = cutoff;
+  return IGPU_OK;
+}
+
+int igpu_get_mixed_cutoffs(const igpu_plan* P, double* cutoff, double* prim_eps) {
+  if (!P) return fail(IGPU_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (cutoff) *cutoff = P->mixed_cutoff;
+  if (prim_eps) *prim_eps = P->mixed_prim_cut;
   return IGPU_OK;
 }
 

@@ -27,12 +27,13 @@ struct igpu_batch {
   // device: densities, J, K (and their one-orientation accumulators), shell
   // bounds, gradient block maxima and output, gradient term tables
   DevBuf<double> d_D, d_J, d_K, d_Jh, d_Kh, d_bounds, d_gmax, d_gout, d_gfac;
+  DevBuf<float> d_Df;  // FP32 copy of the densities (mixed steps)
   DevBuf<const double*> d_gptr;
   // the captured sequence and the arguments it was captured for
   cudaGraphExec_t exec = nullptr;
   bool have_key = false;
-  double key_thr = 0.0, key_cut = 0.0, key_cf = 0.0, key_xf = 0.0;
-  int key_want_k = 0, key_grad = 0, key_sym = 0;
+  double key_thr = 0.0, key_cut = 0.0, key_prim = 0.0, key_cf = 0.0, key_xf = 0.0;
+  int key_want_k = 0, key_grad = 0, key_sym = 0, key_mixed = 0;
   ~igpu_batch() {
     if (exec) cudaGraphExecDestroy(exec);
   }
@@ -45,8 +46,8 @@ size_t blk_len(const igpu_batch* b) { return (size_t)b->nmol * b->S * (b->S + 1)
 
 // The launches of one batch step on stream s, with no host synchronisation
 // and no allocation once the buffers exist (so that it can be captured).
-int enqueue(igpu_batch* b, TaskSet& ts, double threshold, double prim_cut, int want_k, int want_grad, int sym,
-            double cf, double xf, cudaStream_t s, uint32_t& launches) {
+int enqueue(igpu_batch* b, TaskSet& ts, double threshold, int mixed, double prim_cut, int want_k, int want_grad,
+            int sym, double cf, double xf, cudaStream_t s, uint32_t& launches) {
   igpu_plan* P = b->plan.get();
   const size_t ml = mat_len(b);
   CK(cudaMemsetAsync(b->d_J.p, 0, ml * sizeof(double), s));
@@ -61,6 +62,12 @@ int enqueue(igpu_batch* b, TaskSet& ts, double threshold, double prim_cut, int w
   A.jk.symmetric = sym;
   A.jk.threshold = threshold;
   A.prim_cut = prim_cut;
+  if (mixed) {
+    // the FP32 launches read the FP32 copy of the densities
+    CK(launch_to_float(b->d_D.p, b->d_Df.p, ml, s));
+    A.jk.Df = b->d_Df.p;
+    ++launches;
+  }
   if (sym) {
     CK(cudaMemsetAsync(b->d_Jh.p, 0, ml * sizeof(double), s));
     if (want_k) CK(cudaMemsetAsync(b->d_Kh.p, 0, ml * sizeof(double), s));
@@ -332,6 +339,7 @@ int igpu_batch_create(const igpu_shell* sh, const size_t* mol_nsh, size_t nmol, 
   // batch buffers
   const size_t ml = mat_len(b.get()), bl = blk_len(b.get());
   CK(b->d_D.ensure(ml));
+  CK(b->d_Df.ensure(ml));
   CK(b->d_J.ensure(ml));
   CK(b->d_K.ensure(ml));
   CK(b->d_bounds.ensure(bl));
@@ -402,7 +410,9 @@ int igpu_batch_jk_grad(igpu_batch* b, const double* dens, double threshold, int 
   int trc;
   TaskSet* tasks = cached_tasks(P, threshold, fp64_cut, trc);
   if (!tasks) return trc;
-  const bool same = b->have_key && b->key_thr == threshold && b->key_cut == fp64_cut && b->key_want_k == want_k &&
+  const int mixed = precision == IGPU_PRECISION_MIXED ? 1 : 0;
+  const bool same = b->have_key && b->key_thr == threshold && b->key_cut == fp64_cut && b->key_prim == prim_cut &&
+                    b->key_mixed == mixed && b->key_want_k == want_k &&
                     b->key_grad == want_grad && b->key_sym == sym && b->key_cf == coul_factor &&
                     b->key_xf == exch_factor && b->exec;
   uint32_t launches = 0;
@@ -429,13 +439,14 @@ int igpu_batch_jk_grad(igpu_batch* b, const double* dens, double threshold, int 
     }
     // one plain run allocates every scratch buffer; then the same sequence
     // is captured (no allocation or host synchronisation inside it)
-    int rc = enqueue(b, *tasks, threshold, prim_cut, want_k, want_grad, sym, coul_factor, exch_factor, s, launches);
+    int rc = enqueue(b, *tasks, threshold, mixed, prim_cut, want_k, want_grad, sym, coul_factor, exch_factor, s,
+                     launches);
     if (rc) return rc;
     CK(cudaStreamSynchronize(s));
     cudaGraph_t graph = nullptr;
     CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     uint32_t l2 = 0;
-    rc = enqueue(b, *tasks, threshold, prim_cut, want_k, want_grad, sym, coul_factor, exch_factor, s, l2);
+    rc = enqueue(b, *tasks, threshold, mixed, prim_cut, want_k, want_grad, sym, coul_factor, exch_factor, s, l2);
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
     if (rc) {
       if (graph) cudaGraphDestroy(graph);
@@ -448,6 +459,8 @@ int igpu_batch_jk_grad(igpu_batch* b, const double* dens, double threshold, int 
     b->have_key = true;
     b->key_thr = threshold;
     b->key_cut = fp64_cut;
+    b->key_prim = prim_cut;
+    b->key_mixed = mixed;
     b->key_want_k = want_k;
     b->key_grad = want_grad;
     b->key_sym = sym;

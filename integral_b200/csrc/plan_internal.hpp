@@ -158,6 +158,7 @@ struct igpu_plan {
   DevBuf<double> d_schwarz_pair;
   // per-call device buffers
   DevBuf<double> d_D, d_J, d_K, d_bounds, d_dense, d_Jh, d_Kh;
+  DevBuf<float> d_Df;  // FP32 copy of the densities (mixed J/K)
   DevBuf<unsigned long long> d_flag;
   DevBuf<unsigned> d_bitmap;
   std::map<std::pair<double, double>, std::unique_ptr<TaskSet>> jk_tasks;  // (threshold, fp64 cutoff)

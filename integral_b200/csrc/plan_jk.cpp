@@ -72,6 +72,12 @@ int igpu_jk_device(igpu_plan* P, const double* d_dens, int ndens, const uint32_t
   A.prim_cut = prim_cut;
   A.bra_bitmap = bra_subset ? P->d_bitmap.p : nullptr;
   const size_t n2 = (size_t)P->nao * P->nao * ndens;
+  A.jk.Df = nullptr;
+  if (precision == IGPU_PRECISION_MIXED) {
+    CK(P->d_Df.ensure(n2));
+    CK(launch_to_float(d_dens, P->d_Df.p, n2, s));
+    A.jk.Df = P->d_Df.p;
+  }
   if (A.jk.symmetric) {
     // one-orientation accumulators, symmetrised into the caller's J/K below
     CK(P->d_Jh.ensure(n2));

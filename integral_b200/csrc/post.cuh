@@ -200,13 +200,14 @@ struct QuartetCounters {
 // Bra HRR (a, b+1_i | f) = (a+1_i, b | f) + AB_i (a, b | f), i = first
 // nonzero axis of b (src/engine/os_eri.rs:3083-3116), level by level over the
 // whole table; returns the buffer that holds [b][a][f] with a of degree la.
-__device__ __forceinline__ double* hrr_bra(double* buf[3], int& cur, int la, int lb, int nfp, const double ab[3],
-                                           int lane, int T, unsigned tmask) {
+template <typename V>
+__device__ __forceinline__ V* hrr_bra(V* buf[3], int& cur, int la, int lb, int nfp, const double ab[3], int lane,
+                                      int T, unsigned tmask) {
   const int ne = la + lb;
   const int base_a = tri_below(la);
   for (int kb = 1; kb <= lb; ++kb) {
-    const double* src = buf[cur];
-    double* dst = buf[(cur + 1) % 3];
+    const V* src = buf[cur];
+    V* dst = buf[(cur + 1) % 3];
     const int nb_k = ncart(kb);
     const int na_k = nrange(la, ne - kb);
     const int na_p = nrange(la, ne - kb + 1);
@@ -225,9 +226,9 @@ __device__ __forceinline__ double* hrr_bra(double* buf[3], int& cur, int la, int
       const int aaddr = base_a + ia;
       const int ax = addr_lx(aaddr), ay = addr_ly(aaddr), az = addr_lz(aaddr);
       const int ia1 = addr3(ax + (ax_ == 0), ay + (ax_ == 1), az + (ax_ == 2)) - base_a;
-      const double v1 = src[((size_t)ib1 * na_p + ia1) * nfp + f];
-      const double v0 = src[((size_t)ib1 * na_p + ia) * nfp + f];
-      dst[q] = v1 + ab[ax_] * v0;
+      const V v1 = src[((size_t)ib1 * na_p + ia1) * nfp + f];
+      const V v0 = src[((size_t)ib1 * na_p + ia) * nfp + f];
+      dst[q] = v1 + (V)ab[ax_] * v0;
     }
     __syncwarp(tmask);
     cur = (cur + 1) % 3;
@@ -236,13 +237,14 @@ __device__ __forceinline__ double* hrr_bra(double* buf[3], int& cur, int la, int
 }
 
 // Ket HRR per (a,b) row, then the Cartesian block [a][b][c][d].
-__device__ __forceinline__ void hrr_ket(double* buf[3], int hcur, double* blk, int la, int lb, int lc, int ld,
-                                        int nfp, const double cd[3], int lane, int T, unsigned tmask) {
+template <typename V>
+__device__ __forceinline__ void hrr_ket(V* buf[3], int hcur, V* blk, int la, int lb, int lc, int ld, int nfp,
+                                        const double cd[3], int lane, int T, unsigned tmask) {
   const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
   const int nab = na * nb;
   const int nf = lc + ld;
   const int base_c = tri_below(lc);
-  const double* H = buf[hcur];  // [ib][ia][f]
+  const V* H = buf[hcur];  // [ib][ia][f]
   if (ld == 0) {
     const int total = nab * nc;
     for (int q = lane; q < total; q += T) {
@@ -255,9 +257,9 @@ __device__ __forceinline__ void hrr_ket(double* buf[3], int hcur, double* blk, i
   }
   int cur = -1;  // level 0 read from H
   int w0 = (hcur + 1) % 3, w1 = (hcur + 2) % 3;
-  const double* src = H;
+  const V* src = H;
   for (int kd = 1; kd <= ld; ++kd) {
-    double* dst = (kd & 1) ? buf[w0] : buf[w1];
+    V* dst = (kd & 1) ? buf[w0] : buf[w1];
     const int nd_k = ncart(kd);
     const int nc_k = nrange(lc, nf - kd);
     const int nc_p = nrange(lc, nf - kd + 1);
@@ -274,7 +276,7 @@ __device__ __forceinline__ void hrr_ket(double* buf[3], int hcur, double* blk, i
       const int caddr = base_c + ic;
       const int cx = addr_lx(caddr), cy = addr_ly(caddr), cz = addr_lz(caddr);
       const int ic1 = addr3(cx + (jx == 0), cy + (jx == 1), cz + (jx == 2)) - base_c;
-      double v1, v0;
+      V v1, v0;
       if (kd == 1) {
         const int ia = ab / nb, ib = ab % nb;
         const size_t row = ((size_t)ib * na + ia) * nfp;
@@ -284,7 +286,7 @@ __device__ __forceinline__ void hrr_ket(double* buf[3], int hcur, double* blk, i
         v1 = src[((size_t)ab * ncart(kd - 1) + id1) * nc_p + ic1];
         v0 = src[((size_t)ab * ncart(kd - 1) + id1) * nc_p + ic];
       }
-      dst[q] = v1 + cd[jx] * v0;
+      dst[q] = v1 + (V)cd[jx] * v0;
     }
     __syncwarp(tmask);
     src = dst;
@@ -343,6 +345,16 @@ __device__ __forceinline__ double* c2s_block(const KernelArgs& A, double* blk, d
 
 // Shell tuples of the 8 permutations (src/integrals.rs:1235-1244) and which
 // of them are distinct (the reference's dedup by permuted shell tuple).
+// The densities in value type V: the FP64 matrices, or their FP32 copy for
+// the FP32 launches of the mixed path.
+template <typename V>
+__device__ __forceinline__ const V* dens_of(const JKDev& jk) {
+  if constexpr (sizeof(V) == 4)
+    return jk.Df;
+  else
+    return jk.D;
+}
+
 __device__ __forceinline__ unsigned distinct_perms(const int s[4]) {
   const int P[8][4] = {{0, 1, 2, 3}, {1, 0, 2, 3}, {0, 1, 3, 2}, {1, 0, 3, 2},
                        {2, 3, 0, 1}, {2, 3, 1, 0}, {3, 2, 0, 1}, {3, 2, 1, 0}};
@@ -802,27 +814,27 @@ __device__ __forceinline__ void post_quartet(const KernelArgs& A, const ClassDim
 // known at compile time: output (u, v), summed (s, t), D block rows on s and
 // columns on t.  Every sum is fully unrolled, so its block and density loads
 // are independent and in flight together.
-template <int U, int V, int S, int TT, int N0, int N1, int N2, int N3, int T, bool ACC>
-__device__ __forceinline__ void jk_term_ct(const KernelArgs& A, const double* B, const int offs[4], double w, int d0,
-                                           unsigned m, double* out, int lane) {
+template <int U, int V, int S, int TT, int N0, int N1, int N2, int N3, int T, bool ACC, typename X>
+__device__ __forceinline__ void jk_term_ct(const KernelArgs& A, const X* B, const int offs[4], X w, int d0, unsigned m,
+                                           double* out, int lane) {
   constexpr int N[4] = {N0, N1, N2, N3};
   constexpr int ST[4] = {N1 * N2 * N3, N2 * N3, N3, 1};
   constexpr int NU = N[U], NV = N[V], NS = N[S], NT = N[TT];
   constexpr int DCH = JK_DCH;
   const int nao = A.nao;
   const size_t n2 = (size_t)nao * nao;
-  const double* Dp = A.jk.D + (size_t)d0 * n2 + (size_t)offs[S] * nao + offs[TT];
+  const X* Dp = dens_of<X>(A.jk) + (size_t)d0 * n2 + (size_t)offs[S] * nao + offs[TT];
   for (int r = lane; r < NU * NV; r += T) {
     const int iu = r / NV, iv = r - (r / NV) * NV;
-    const double* Bp = B + iu * ST[U] + iv * ST[V];
-    double sum[DCH];
+    const X* Bp = B + iu * ST[U] + iv * ST[V];
+    X sum[DCH];
 #pragma unroll
-    for (int k = 0; k < DCH; ++k) sum[k] = 0.0;
+    for (int k = 0; k < DCH; ++k) sum[k] = X(0);
 #pragma unroll
     for (int is = 0; is < NS; ++is)
 #pragma unroll
       for (int it = 0; it < NT; ++it) {
-        const double b = Bp[is * ST[S] + it * ST[TT]];
+        const X b = Bp[is * ST[S] + it * ST[TT]];
 #pragma unroll
         for (int k = 0; k < DCH; ++k)
           if ((m >> k) & 1u) sum[k] += b * __ldg(Dp + k * n2 + (size_t)is * nao + it);
@@ -830,13 +842,182 @@ __device__ __forceinline__ void jk_term_ct(const KernelArgs& A, const double* B,
     if (ACC) {
 #pragma unroll
       for (int k = 0; k < DCH; ++k)
-        if ((m >> k) & 1u) out[1 + (size_t)(d0 + k) * (N0 * N1) + r] += w * sum[k];
+        if ((m >> k) & 1u) out[1 + (size_t)(d0 + k) * (N0 * N1) + r] += (double)(w * sum[k]);
     } else {
       const size_t o = (size_t)(offs[U] + iu) * nao + offs[V] + iv;
 #pragma unroll
       for (int k = 0; k < DCH; ++k)
-        if ((m >> k) & 1u) atomicAdd(out + (size_t)(d0 + k) * n2 + o, w * sum[k]);
+        if ((m >> k) & 1u) atomicAdd(out + (size_t)(d0 + k) * n2 + o, (double)(w * sum[k]));
     }
+  }
+}
+
+// Index tables of the team horizontal recurrences of one class, built once
+// per block in shared memory: one entry per element of a bra level (b, a) or
+// a ket level (d, c), packing the two source rows of the recurrence (bits
+// 0-10 and 11-21, within the previous level), its axis (22-23) and, on the
+// last ket level, the element's place in the [c][d] block row (24-31).  The
+// loops then spend a shared-memory load per element instead of the
+// component arithmetic.
+template <int LA, int LB, int LC, int LD>
+struct HrrTab {
+  static constexpr int NE = LA + LB, NF = LC + LD;
+  static __host__ __device__ constexpr int bra_off(int kb) {
+    int o = 0;
+    for (int k = 1; k < kb; ++k) o += ncart(k) * nrange(LA, NE - k);
+    return o;
+  }
+  static __host__ __device__ constexpr int ket_off(int kd) {
+    int o = bra_off(LB + 1);
+    for (int k = 1; k < kd; ++k) o += ncart(k) * nrange(LC, NF - k);
+    return o;
+  }
+  static constexpr int TOTAL = ket_off(LD + 1) > 0 ? ket_off(LD + 1) : 1;
+};
+
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void build_hrr_tab(int* tab) {
+  using H = HrrTab<LA, LB, LC, LD>;
+  constexpr int NE = H::NE, NF = H::NF;
+  for (int t = threadIdx.x; t < H::TOTAL; t += blockDim.x) {
+    if (t >= H::ket_off(LD + 1)) break;
+    int v = 0;
+    if (t < H::bra_off(LB + 1)) {
+      int kb = 1;
+      while (t >= H::bra_off(kb + 1)) ++kb;
+      const int el = t - H::bra_off(kb);
+      const int nak = nrange(LA, NE - kb), nap = nrange(LA, NE - kb + 1);
+      const int ib = el / nak, ia = el % nak;
+      const int baddr = tri_below(kb) + ib;
+      const int bx = addr_lx(baddr), by = addr_ly(baddr), bz = addr_lz(baddr);
+      const int ax = bx > 0 ? 0 : (by > 0 ? 1 : 2);
+      const int ib1 = cart_index3(bx - (ax == 0), by - (ax == 1), bz - (ax == 2));
+      const int aaddr = tri_below(LA) + ia;
+      const int px = addr_lx(aaddr), py = addr_ly(aaddr), pz = addr_lz(aaddr);
+      const int ia1 = addr3(px + (ax == 0), py + (ax == 1), pz + (ax == 2)) - tri_below(LA);
+      v = (ib1 * nap + ia1) | ((ib1 * nap + ia) << 11) | (ax << 22);
+    } else {
+      int kd = 1;
+      while (t >= H::ket_off(kd + 1)) ++kd;
+      const int el = t - H::ket_off(kd);
+      const int nck = nrange(LC, NF - kd), ncp = nrange(LC, NF - kd + 1);
+      const int id = el / nck, ic = el % nck;
+      const int daddr = tri_below(kd) + id;
+      const int dx = addr_lx(daddr), dy = addr_ly(daddr), dz = addr_lz(daddr);
+      const int jx = dx > 0 ? 0 : (dy > 0 ? 1 : 2);
+      const int id1 = cart_index3(dx - (jx == 0), dy - (jx == 1), dz - (jx == 2));
+      const int caddr = tri_below(LC) + ic;
+      const int cx = addr_lx(caddr), cy = addr_ly(caddr), cz = addr_lz(caddr);
+      const int ic1 = addr3(cx + (jx == 0), cy + (jx == 1), cz + (jx == 2)) - tri_below(LC);
+      const int dpos = ic * ncart(LD) + id;  // place in the block row (last level)
+      v = (id1 * ncp + ic1) | ((id1 * ncp + ic) << 11) | (jx << 22) | (dpos << 24);
+    }
+    tab[t] = v;
+  }
+}
+
+template <typename X>
+__device__ __forceinline__ X pick_axis(int ax, const X v[3]) {
+  return ax == 0 ? v[0] : (ax == 1 ? v[1] : v[2]);
+}
+
+// The horizontal recurrences of one quartet on a team, table driven (same
+// recurrences and order as hrr_bra / hrr_ket): the [e0|f0] table in buf[0]
+// ([e][f]) becomes the Cartesian block [a][b][c][d] in `out`.
+template <int LA, int LB, int LC, int LD, int T, typename X>
+__device__ __forceinline__ void team_hrr(X* buf[3], const int* tab, X* out, const double ab[3], const double cd[3],
+                                         int lane, unsigned tmask) {
+  using H = HrrTab<LA, LB, LC, LD>;
+  constexpr int NE = H::NE, NF = H::NF;
+  constexpr int NFP = nrange(LC, NF);
+  constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+  constexpr int NAB = NA * NB;
+  const X abv[3] = {(X)ab[0], (X)ab[1], (X)ab[2]};
+  const X cdv[3] = {(X)cd[0], (X)cd[1], (X)cd[2]};
+  int cur = 0;
+  static_for<LB>([&](auto k_) {
+    constexpr int KB = decltype(k_)::value + 1;
+    constexpr int N = ncart(KB) * nrange(LA, NE - KB) * NFP;
+    constexpr int OFF = H::bra_off(KB);
+    const X* src = buf[cur];
+    X* dst = buf[(cur + 1) % 3];
+    for (int q = lane; q < N; q += T) {
+      const int row = q / NFP, f = q - row * NFP;
+      const int e = tab[OFF + row];
+      dst[q] = src[(e & 0x7ff) * NFP + f] + pick_axis(e >> 22 & 3, abv) * src[((e >> 11) & 0x7ff) * NFP + f];
+    }
+    __syncwarp(tmask);
+    cur = (cur + 1) % 3;
+  });
+  const X* Hb = buf[cur];  // [b][a][f]
+  if constexpr (LD == 0) {
+    for (int q = lane; q < NAB * NC; q += T) {
+      const int abr = q / NC, ic = q - abr * NC;
+      const int ia = abr / NB, ib = abr - ia * NB;
+      out[q] = Hb[(ib * NA + ia) * NFP + ic];
+    }
+  } else {
+    const int w0 = (cur + 1) % 3, w1 = (cur + 2) % 3;
+    static_for<LD>([&](auto k_) {
+      constexpr int KD = decltype(k_)::value + 1;
+      constexpr int NEL = ncart(KD) * nrange(LC, NF - KD);
+      constexpr int NELP = ncart(KD - 1) * nrange(LC, NF - KD + 1);
+      constexpr int OFF = H::ket_off(KD);
+      const X* src = KD == 1 ? Hb : ((KD & 1) ? buf[w1] : buf[w0]);
+      X* dst = (KD & 1) ? buf[w0] : buf[w1];
+      for (int q = lane; q < NAB * NEL; q += T) {
+        const int abr = q / NEL, el = q - abr * NEL;
+        const int e = tab[OFF + el];
+        int base;
+        if constexpr (KD == 1) {
+          const int ia = abr / NB, ib = abr - ia * NB;
+          base = (ib * NA + ia) * NFP;
+        } else {
+          base = abr * NELP;
+        }
+        const X v = src[base + (e & 0x7ff)] + pick_axis(e >> 22 & 3, cdv) * src[base + ((e >> 11) & 0x7ff)];
+        if constexpr (KD == LD)
+          out[abr * (NC * ND) + ((e >> 24) & 0xff)] = v;
+        else
+          dst[q] = v;
+      }
+      __syncwarp(tmask);
+    });
+  }
+  __syncwarp(tmask);
+}
+
+// One axis of the Cartesian -> spherical transform of a [D0][D1][D2][D3]
+// block on a team (same sums as c2s_axis): M is the (2l+1) x n_cart matrix
+// in shared memory.
+template <int AXIS, int D0, int D1, int D2, int D3, int NOUT, int T, typename X>
+__device__ __forceinline__ void team_c2s_axis(const X* in, X* out, const X* M, int lane) {
+  constexpr int dims[4] = {D0, D1, D2, D3};
+  constexpr int NIN = dims[AXIS];
+  constexpr int outer = AXIS == 0 ? 1 : (AXIS == 1 ? D0 : (AXIS == 2 ? D0 * D1 : D0 * D1 * D2));
+  constexpr int inner = AXIS == 0 ? D1 * D2 * D3 : (AXIS == 1 ? D2 * D3 : (AXIS == 2 ? D3 : 1));
+  for (int q = lane; q < outer * NOUT * inner; q += T) {
+    const int sidx = q % inner, t = q / inner;
+    const int qo = t % NOUT, o = t / NOUT;
+    const X* src = in + (o * NIN) * inner + sidx;
+    const X* m = M + qo * NIN;
+    X acc = X(0);
+#pragma unroll
+    for (int j = 0; j < NIN; ++j) acc += m[j] * src[j * inner];
+    out[q] = acc;
+  }
+}
+
+// Shared-memory copies of the four c2s matrices of a class (l_a, l_b, l_c,
+// l_d), rows of at most 7 x 10.
+constexpr int C2S_TILE = 70;
+template <int LA, int LB, int LC, int LD, typename X>
+__device__ __forceinline__ void stage_c2s(const KernelArgs& A, X* s_m) {
+  const int ls[4] = {LA, LB, LC, LD};
+  for (int t = threadIdx.x; t < 4 * C2S_TILE; t += blockDim.x) {
+    const int ax = t / C2S_TILE, i = t - ax * C2S_TILE;
+    const int l = ls[ax];
+    s_m[t] = i < (2 * l + 1) * ncart(l) ? (X)A.c2s[A.c2s_off[l] + i] : X(0);
   }
 }
 
@@ -844,26 +1025,19 @@ __device__ __forceinline__ void jk_term_ct(const KernelArgs& A, const double* B,
 // horizontal recurrences into the slot, the block copied to the team's
 // shared memory (when it has room), then the six image contractions of
 // consume_jk with the shape fixed at compile time.
-template <int LA, int LB, int LC, int LD, int T>
+template <int LA, int LB, int LC, int LD, int T, typename X>
 __device__ __forceinline__ void post_quartet_jk_cart(const KernelArgs& A, const PairD& pb, const PairD& pk,
                                                      const Screen& sc, double* slot, int lane, unsigned tmask, int pbi,
-                                                     double* stage) {
+                                                     X* stage, const int* hrr_tab) {
   constexpr int N0 = ncart(LA), N1 = ncart(LB), N2 = ncart(LC), N3 = ncart(LD);
-  constexpr int NBLK = N0 * N1 * N2 * N3;
   const SlotLayout L = slot_layout(LA, LB, LC, LD);
-  double* buf[3] = {slot, slot + L.S, slot + 2 * L.S};
-  double* blk = slot + 3 * L.S;
+  X* xs = reinterpret_cast<X*>(slot);
+  X* buf[3] = {xs, xs + L.S, xs + 2 * L.S};
   const double ab[3] = {pb.abx, pb.aby, pb.abz};
   const double cdv[3] = {pk.abx, pk.aby, pk.abz};
-  int cur = 0;
-  hrr_bra(buf, cur, LA, LB, nrange(LC, LC + LD), ab, lane, T, tmask);
-  hrr_ket(buf, cur, blk, LA, LB, LC, LD, nrange(LC, LC + LD), cdv, lane, T, tmask);
-  const double* B = blk;
-  if (stage) {
-    for (int q = lane; q < NBLK; q += T) stage[q] = blk[q];
-    __syncwarp(tmask);
-    B = stage;
-  }
+  // the block goes straight to the team's shared memory when it has room
+  X* B = stage ? stage : xs + 3 * L.S;
+  team_hrr<LA, LB, LC, LD, T, X>(buf, hrr_tab, B, ab, cdv, lane, tmask);
   const int shl[4] = {pb.a, pb.b, pk.a, pk.b};
   const int offs[4] = {A.shells[shl[0]].off, A.shells[shl[1]].off, A.shells[shl[2]].off, A.shells[shl[3]].off};
   double* acc = slot + A.acc_offset;
@@ -873,21 +1047,77 @@ __device__ __forceinline__ void post_quartet_jk_cart(const KernelArgs& A, const 
     __syncwarp(tmask);
   }
   const unsigned wp = distinct_perms(shl);
-  auto W = [&](int p) { return (double)((wp >> p) & 1u); };
-  const double w0 = W(0) + W(1) + W(2) + W(3), w1 = W(4) + W(5) + W(6) + W(7);
-  const double w2 = W(0) + W(4), w3 = W(1) + W(5), w4 = W(2) + W(6), w5 = W(3) + W(7);
+  auto W = [&](int p) { return (X)((wp >> p) & 1u); };
+  const X w0 = W(0) + W(1) + W(2) + W(3), w1 = W(4) + W(5) + W(6) + W(7);
+  const X w2 = W(0) + W(4), w3 = W(1) + W(5), w4 = W(2) + W(6), w5 = W(3) + W(7);
   const unsigned long long live = A.jk.ndens >= 64 ? ~0ull : ((1ull << A.jk.ndens) - 1ull);
   const uint64_t mask = sc.mask & live;
   for (int d0 = 0; d0 < A.jk.ndens; d0 += JK_DCH) {
     const unsigned m = (unsigned)((mask >> d0) & ((1u << JK_DCH) - 1u));
     if (!m) continue;
-    jk_term_ct<0, 1, 2, 3, N0, N1, N2, N3, T, true>(A, B, offs, w0, d0, m, acc, lane);
-    if (w1 != 0.0) jk_term_ct<2, 3, 0, 1, N0, N1, N2, N3, T, false>(A, B, offs, w1, d0, m, A.jk.J, lane);
+    jk_term_ct<0, 1, 2, 3, N0, N1, N2, N3, T, true, X>(A, B, offs, w0, d0, m, acc, lane);
+    if (w1 != X(0)) jk_term_ct<2, 3, 0, 1, N0, N1, N2, N3, T, false, X>(A, B, offs, w1, d0, m, A.jk.J, lane);
     if (A.jk.want_k) {
-      if (w2 != 0.0) jk_term_ct<0, 2, 1, 3, N0, N1, N2, N3, T, false>(A, B, offs, w2, d0, m, A.jk.K, lane);
-      if (w3 != 0.0) jk_term_ct<1, 2, 0, 3, N0, N1, N2, N3, T, false>(A, B, offs, w3, d0, m, A.jk.K, lane);
-      if (w4 != 0.0) jk_term_ct<0, 3, 1, 2, N0, N1, N2, N3, T, false>(A, B, offs, w4, d0, m, A.jk.K, lane);
-      if (w5 != 0.0) jk_term_ct<1, 3, 0, 2, N0, N1, N2, N3, T, false>(A, B, offs, w5, d0, m, A.jk.K, lane);
+      if (w2 != X(0)) jk_term_ct<0, 2, 1, 3, N0, N1, N2, N3, T, false, X>(A, B, offs, w2, d0, m, A.jk.K, lane);
+      if (w3 != X(0)) jk_term_ct<1, 2, 0, 3, N0, N1, N2, N3, T, false, X>(A, B, offs, w3, d0, m, A.jk.K, lane);
+      if (w4 != X(0)) jk_term_ct<0, 3, 1, 2, N0, N1, N2, N3, T, false, X>(A, B, offs, w4, d0, m, A.jk.K, lane);
+      if (w5 != X(0)) jk_term_ct<1, 3, 0, 2, N0, N1, N2, N3, T, false, X>(A, B, offs, w5, d0, m, A.jk.K, lane);
+    }
+  }
+  __syncwarp(tmask);
+}
+
+// Post phase of a symmetric J/K quartet whose four shells are spherical:
+// table-driven horizontal recurrences into the slot, the four transform
+// axes on the team, the spherical block in the team's shared memory when it
+// has room, then the six image contractions with the spherical shape.
+template <int LA, int LB, int LC, int LD, int T, typename X>
+__device__ __forceinline__ void post_quartet_jk_sph(const KernelArgs& A, const PairD& pb, const PairD& pk,
+                                                    const Screen& sc, double* slot, int lane, unsigned tmask, int pbi,
+                                                    X* stage, const int* hrr_tab, const X* s_m) {
+  constexpr int N0 = ncart(LA), N1 = ncart(LB), N2 = ncart(LC), N3 = ncart(LD);
+  constexpr int F0 = 2 * LA + 1, F1 = 2 * LB + 1, F2 = 2 * LC + 1, F3 = 2 * LD + 1;
+  const SlotLayout L = slot_layout(LA, LB, LC, LD);
+  X* xs = reinterpret_cast<X*>(slot);
+  X* buf[3] = {xs, xs + L.S, xs + 2 * L.S};
+  X* blk = xs + 3 * L.S;
+  X* tmp = blk + L.blk;
+  const double ab[3] = {pb.abx, pb.aby, pb.abz};
+  const double cdv[3] = {pk.abx, pk.aby, pk.abz};
+  team_hrr<LA, LB, LC, LD, T, X>(buf, hrr_tab, blk, ab, cdv, lane, tmask);
+  team_c2s_axis<0, N0, N1, N2, N3, F0, T, X>(blk, tmp, s_m + 0 * C2S_TILE, lane);
+  __syncwarp(tmask);
+  team_c2s_axis<1, F0, N1, N2, N3, F1, T, X>(tmp, blk, s_m + 1 * C2S_TILE, lane);
+  __syncwarp(tmask);
+  team_c2s_axis<2, F0, F1, N2, N3, F2, T, X>(blk, tmp, s_m + 2 * C2S_TILE, lane);
+  __syncwarp(tmask);
+  X* B = stage ? stage : blk;
+  team_c2s_axis<3, F0, F1, F2, N3, F3, T, X>(tmp, B, s_m + 3 * C2S_TILE, lane);
+  __syncwarp(tmask);
+  const int shl[4] = {pb.a, pb.b, pk.a, pk.b};
+  const int offs[4] = {A.shells[shl[0]].off, A.shells[shl[1]].off, A.shells[shl[2]].off, A.shells[shl[3]].off};
+  double* acc = slot + A.acc_offset;
+  if ((int)acc[0] != pbi) {
+    flush_bra_acc(A, acc, lane, T, tmask);
+    if (lane == 0) acc[0] = (double)pbi;
+    __syncwarp(tmask);
+  }
+  const unsigned wp = distinct_perms(shl);
+  auto W = [&](int p) { return (X)((wp >> p) & 1u); };
+  const X w0 = W(0) + W(1) + W(2) + W(3), w1 = W(4) + W(5) + W(6) + W(7);
+  const X w2 = W(0) + W(4), w3 = W(1) + W(5), w4 = W(2) + W(6), w5 = W(3) + W(7);
+  const unsigned long long live = A.jk.ndens >= 64 ? ~0ull : ((1ull << A.jk.ndens) - 1ull);
+  const uint64_t mask = sc.mask & live;
+  for (int d0 = 0; d0 < A.jk.ndens; d0 += JK_DCH) {
+    const unsigned m = (unsigned)((mask >> d0) & ((1u << JK_DCH) - 1u));
+    if (!m) continue;
+    jk_term_ct<0, 1, 2, 3, F0, F1, F2, F3, T, true, X>(A, B, offs, w0, d0, m, acc, lane);
+    if (w1 != X(0)) jk_term_ct<2, 3, 0, 1, F0, F1, F2, F3, T, false, X>(A, B, offs, w1, d0, m, A.jk.J, lane);
+    if (A.jk.want_k) {
+      if (w2 != X(0)) jk_term_ct<0, 2, 1, 3, F0, F1, F2, F3, T, false, X>(A, B, offs, w2, d0, m, A.jk.K, lane);
+      if (w3 != X(0)) jk_term_ct<1, 2, 0, 3, F0, F1, F2, F3, T, false, X>(A, B, offs, w3, d0, m, A.jk.K, lane);
+      if (w4 != X(0)) jk_term_ct<0, 3, 1, 2, F0, F1, F2, F3, T, false, X>(A, B, offs, w4, d0, m, A.jk.K, lane);
+      if (w5 != X(0)) jk_term_ct<1, 3, 0, 2, F0, F1, F2, F3, T, false, X>(A, B, offs, w5, d0, m, A.jk.K, lane);
     }
   }
   __syncwarp(tmask);

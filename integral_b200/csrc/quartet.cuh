@@ -206,7 +206,7 @@ __device__ __forceinline__ void rys_root_one(const R* s_tab, R T, int r, R& x, R
 template <int LA, int LB, int LC, int LD, typename R, int F0>
 __device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, const PairD& pb, const PairD& pk,
                                           R* sm, int lane, unsigned tmask, double* G, const unsigned short* surv,
-                                          int npr) {
+                                          int npr, bool g32) {
   using S = ClassShape<LA, LB, LC, LD>;
   using TS = TeamShape<LA, LB, LC, LD, R>;
   constexpr int NE = S::NE, NF = S::NF, NR = S::NR, T = TS::T;
@@ -327,8 +327,15 @@ __device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, c
   for (int k = 0; k < TS::ROWS; ++k) {
     int e = lane + T * k;
     if (e < S::NEP) {
+      if (sizeof(R) == 4 && g32) {
+        // FP32 post phase: the table stays in FP32
+        float* Gf = reinterpret_cast<float*>(G);
 #pragma unroll
-      for (int f = 0; f < FW; ++f) G[(size_t)e * S::NFP + F0 + f] = (double)acc[k][f];
+        for (int f = 0; f < FW; ++f) Gf[(size_t)e * S::NFP + F0 + f] = (float)acc[k][f];
+      } else {
+#pragma unroll
+        for (int f = 0; f < FW; ++f) G[(size_t)e * S::NFP + F0 + f] = (double)acc[k][f];
+      }
     }
   }
 }
@@ -336,12 +343,12 @@ __device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, c
 template <int LA, int LB, int LC, int LD, typename R, int C>
 __device__ __forceinline__ void team_chunks(const KernelArgs& A, const R* s_tab, const PairD& pb, const PairD& pk,
                                             R* sm, int lane, unsigned tmask, double* G, const unsigned short* surv,
-                                            int npr) {
+                                            int npr, bool g32) {
   using TS = TeamShape<LA, LB, LC, LD, R>;
   if constexpr (C < TS::NCHUNK) {
-    team_pass<LA, LB, LC, LD, R, C * TS::FCH>(A, s_tab, pb, pk, sm, lane, tmask, G, surv, npr);
+    team_pass<LA, LB, LC, LD, R, C * TS::FCH>(A, s_tab, pb, pk, sm, lane, tmask, G, surv, npr, g32);
     __syncwarp(tmask);
-    team_chunks<LA, LB, LC, LD, R, C + 1>(A, s_tab, pb, pk, sm, lane, tmask, G, surv, npr);
+    team_chunks<LA, LB, LC, LD, R, C + 1>(A, s_tab, pb, pk, sm, lane, tmask, G, surv, npr, g32);
   }
 }
 
@@ -395,7 +402,14 @@ __global__ void __launch_bounds__(128, quartet_min_blocks<LA, LB, LC, LD, R>()) 
   __shared__ R s_tab[S::NR * RYS_MAX_SUB * 2 * RYS_NC];
   constexpr bool SCREEN = sizeof(R) == 4 && T > 1;
   __shared__ unsigned short s_surv[SCREEN ? (128 / T) * MAX_SURV : 1];
-  stage_rys_table<S::NR, R>(s_tab);
+  constexpr bool CT_POST = ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD) <= 10000;
+  __shared__ int s_hrr[(T > 1 && CT_POST) ? HrrTab<LA, LB, LC, LD>::TOTAL : 1];
+  __shared__ R s_c2s[(T > 1 && CT_POST) ? 4 * C2S_TILE : 1];
+  if constexpr (T > 1 && CT_POST) {
+    build_hrr_tab<LA, LB, LC, LD>(s_hrr);
+    stage_c2s<LA, LB, LC, LD, R>(A, s_c2s);
+  }
+  stage_rys_table<S::NR, R>(s_tab);  // its __syncthreads also publishes s_hrr, s_c2s
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int team = tid / T;
   const int lane = threadIdx.x % T;
@@ -404,6 +418,7 @@ __global__ void __launch_bounds__(128, quartet_min_blocks<LA, LB, LC, LD, R>()) 
   unsigned char* team_smem = smem_raw + (size_t)(threadIdx.x / T) * TS::TEAM_BYTES;
   R* sm = reinterpret_cast<R*>(team_smem);
   double* stage = TS::STAGE ? reinterpret_cast<double*>(team_smem) : nullptr;
+  R* stage_r = TS::STAGE ? reinterpret_cast<R*>(team_smem) : nullptr;
   double* slot = A.scratch + (size_t)team * A.slot_doubles;
   QuartetCounters cnt;
   const ClassDims dims{LA, LB, LC, LD};
@@ -444,13 +459,12 @@ __global__ void __launch_bounds__(128, quartet_min_blocks<LA, LB, LC, LD, R>()) 
         R G[S::NG];
         accumulate_thread<LA, LB, LC, LD, R>(A, s_tab, pb, pk, G);
         if (use_acc && A.kinds != 2) {
-          double Gd[S::NG];
-#pragma unroll
-          for (int q = 0; q < S::NG; ++q) Gd[q] = (double)G[q];
+          // the post phase runs in the launch's arithmetic (FP32 launches
+          // read the FP32 densities); J/K accumulate in FP64
           if (A.kinds == 0)
-            thread_post_jk<LA, LB, LC, LD, false>(A, Gd, pb, pk, sc, slot + A.acc_offset, pbi);
+            thread_post_jk<LA, LB, LC, LD, false, R>(A, G, pb, pk, sc, slot + A.acc_offset, pbi);
           else
-            thread_post_jk<LA, LB, LC, LD, true>(A, Gd, pb, pk, sc, slot + A.acc_offset, pbi);
+            thread_post_jk<LA, LB, LC, LD, true, R>(A, G, pb, pk, sc, slot + A.acc_offset, pbi);
           continue;
         }
 #pragma unroll
@@ -466,15 +480,20 @@ __global__ void __launch_bounds__(128, quartet_min_blocks<LA, LB, LC, LD, R>()) 
             if (npr == 0) continue;  // the whole quartet is below the screen
           }
         }
-        team_chunks<LA, LB, LC, LD, R, 0>(A, s_tab, pb, pk, sm, lane, tmask, slot, surv, npr);
+        team_chunks<LA, LB, LC, LD, R, 0>(A, s_tab, pb, pk, sm, lane, tmask, slot, surv, npr,
+                                          CT_POST && use_acc && A.kinds != 2);
       }
       __syncwarp(tmask);
       // the compile-time shaped J/K sums unroll over the whole Cartesian
-      // block; blocks beyond (ff|ff) (g shells) take the runtime post phase
-      constexpr bool CT_POST = ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD) <= 10000;
+      // block, in the launch's arithmetic; blocks beyond (ff|ff) (g shells)
+      // take the runtime post phase
       if constexpr (T > 1 && CT_POST) {
         if (use_acc && A.kinds == 0) {
-          post_quartet_jk_cart<LA, LB, LC, LD, T>(A, pb, pk, sc, slot, lane, tmask, pbi, stage);
+          post_quartet_jk_cart<LA, LB, LC, LD, T, R>(A, pb, pk, sc, slot, lane, tmask, pbi, stage_r, s_hrr);
+          continue;
+        }
+        if (use_acc && A.kinds == 1) {
+          post_quartet_jk_sph<LA, LB, LC, LD, T, R>(A, pb, pk, sc, slot, lane, tmask, pbi, stage_r, s_hrr, s_c2s);
           continue;
         }
       }

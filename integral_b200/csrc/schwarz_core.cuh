@@ -2,11 +2,12 @@
 // the device: the same arithmetic, in the same order, as the host evaluation
 // (host_schwarz.cpp) and the reference (src/engine/os_eri.rs:455-697,
 // 2860-3143, src/math/boys.rs:63-431, src/spherical.rs:121-179), so that the
-// device produces the reference's Schwarz bounds bit for bit.  One thread
-// evaluates one shell pair; its work arrays live in a per-thread slice of a
-// global scratch buffer, element k at base[k * stride] (stride = threads of
-// the launch, so that the threads of a warp, which run the same class,
-// touch consecutive words).  The vertical recurrence keeps the reference's
+// device produces the reference's Schwarz bounds bit for bit.  One thread,
+// or one warp for the larger classes, evaluates one shell pair; its work
+// arrays live in a slice of a global scratch buffer, element k at
+// base[k * stride] (one thread per pair: stride = threads of the launch, so
+// that the threads of a warp touch consecutive words; one warp per pair:
+// stride 1, the lanes splitting each level).  The vertical recurrence keeps the reference's
 // rolling window of three ket levels, each packed by Boys order.  Compile
 // with -fmad=false: every product and sum rounds on its own, as in Rust.
 #pragma once
@@ -108,15 +109,38 @@ struct SClass {
 };
 
 
-// One thread's (ij|ij): shells given by centre, l, primitive count,
+// The lanes that evaluate one pair together: lane in [0, size), size 1 or
+// a full warp.  Every element of a recurrence level, of a transform axis and
+// of a contracted table is computed by one lane with the operations of the
+// serial order (the primitive loops stay sequential and every sum keeps its
+// order), so any team size gives the same bits; sync() separates the
+// phases that read what other lanes wrote.
+struct Team {
+  int lane, size;
+  SC_HD void sync() const {
+#ifdef __CUDA_ARCH__
+    if (size > 1) __syncwarp();
+#endif
+  }
+};
+
+// Degree of the Cartesian address a (sc_deg_below(d) <= a < sc_deg_below(d + 1)).
+SC_HD int sc_degree(int a) {
+  int d = 0;
+  while (sc_deg_below(d + 1) <= a) ++d;
+  return d;
+}
+
+// (ij|ij) of one team: shells given by centre, l, primitive count,
 // exponents, effective coefficients and c2s matrix (nullptr: Cartesian);
 // kappa = the host's exp(-(e1 e2 / z) |AB|^2) of every (i, j) primitive
-// combination, i outer.  Returns Q = sqrt(max |(mu nu|mu nu)|).
-SC_HD double sc_schwarz(const BoysDev& B, const SClass& C, const Slice& W, const double* ca, const double* cb,
-                        int npa, int npb, const double* ea, const double* wa, const double* eb,
+// combination, i outer.  Returns Q = sqrt(max |(mu nu|mu nu)|) on every lane.
+SC_HD double sc_schwarz(const BoysDev& B, const SClass& C, const Slice& W, const Team& T, const double* ca,
+                        const double* cb, int npa, int npb, const double* ea, const double* wa, const double* eb,
                         const double* wb, const double* kappa, const double* c2a, const double* c2b) {
   const int la = C.li, lb = C.lj;
   const int ne = C.ne, nf = C.nf, lt = C.lt, n_e = C.n_e, n_f = C.n_f;
+  const int L0 = T.lane, LS = T.size;
   // primitive pairs (src/engine/os_eri.rs:221-244), 11 doubles each
   int np = 0;
   for (int a = 0; a < npa; ++a)
@@ -126,45 +150,52 @@ SC_HD double sc_schwarz(const BoysDev& B, const SClass& C, const Slice& W, const
       const double z = e1 + e2;
       const double kap = kappa[a * npb + b];
       if (kap * fabs(c1 * c2) < 1e-32) continue;
-      const size_t o = C.o_prims + (size_t)np * 11;
-      W[o + 0] = z;
-      W[o + 1] = kap;
-      W[o + 2] = c1;
-      W[o + 3] = c2;
-      W[o + 4] = 0.5 / z;
-      for (int k = 0; k < 3; ++k) {
-        const double P = (e1 * ca[k] + e2 * cb[k]) / z;
-        W[o + 5 + k] = P;
-        W[o + 8 + k] = P - ca[k];
+      if (L0 == 0) {
+        const size_t o = C.o_prims + (size_t)np * 11;
+        W[o + 0] = z;
+        W[o + 1] = kap;
+        W[o + 2] = c1;
+        W[o + 3] = c2;
+        W[o + 4] = 0.5 / z;
+        for (int k = 0; k < 3; ++k) {
+          const double P = (e1 * ca[k] + e2 * cb[k]) / z;
+          W[o + 5 + k] = P;
+          W[o + 8 + k] = P - ca[k];
+        }
       }
       ++np;
     }
   const int na = sc_ncart(la), nb = sc_ncart(lb);
   const size_t nblk = (size_t)na * nb * na * nb;
-  for (size_t q = 0; q < nblk; ++q) W[C.o_blk + q] = 0.0;
+  for (size_t q = L0; q < nblk; q += LS) W[C.o_blk + q] = 0.0;
+  T.sync();
   if (lt == 0) {
     // (ss|ss) fast path (src/engine/os_eri.rs:500-536)
-    const double two_pi_2_5 = 2.0 * kPi * kPi * ::sqrt(kPi);
-    double acc = 0.0;
-    for (int x = 0; x < np; ++x) {
-      const size_t ob = C.o_prims + (size_t)x * 11;
-      const double bc = W[ob + 2] * W[ob + 3];
-      const double p = W[ob + 0];
-      for (int y = 0; y < np; ++y) {
-        const size_t ok = C.o_prims + (size_t)y * 11;
-        const double q = W[ok + 0];
-        const double pq = p + q;
-        const double dx = W[ob + 5] - W[ok + 5], dy = W[ob + 6] - W[ok + 6], dz = W[ob + 7] - W[ok + 7];
-        const double t = (p * q / pq) * (dx * dx + dy * dy + dz * dz);
-        const double pref = two_pi_2_5 / (p * q * ::sqrt(pq)) * W[ob + 1] * W[ok + 1];
-        double f0;
-        sc_boys(B, 0, t, &f0);
-        acc += (bc * W[ok + 2]) * W[ok + 3] * (pref * f0);
+    if (L0 == 0) {
+      const double two_pi_2_5 = 2.0 * kPi * kPi * ::sqrt(kPi);
+      double acc = 0.0;
+      for (int x = 0; x < np; ++x) {
+        const size_t ob = C.o_prims + (size_t)x * 11;
+        const double bc = W[ob + 2] * W[ob + 3];
+        const double p = W[ob + 0];
+        for (int y = 0; y < np; ++y) {
+          const size_t ok = C.o_prims + (size_t)y * 11;
+          const double q = W[ok + 0];
+          const double pq = p + q;
+          const double dx = W[ob + 5] - W[ok + 5], dy = W[ob + 6] - W[ok + 6], dz = W[ob + 7] - W[ok + 7];
+          const double t = (p * q / pq) * (dx * dx + dy * dy + dz * dz);
+          const double pref = two_pi_2_5 / (p * q * ::sqrt(pq)) * W[ob + 1] * W[ok + 1];
+          double f0;
+          sc_boys(B, 0, t, &f0);
+          acc += (bc * W[ok + 2]) * W[ok + 3] * (pref * f0);
+        }
       }
+      W[C.o_blk] += acc;
     }
-    W[C.o_blk] += acc;
+    T.sync();
   } else {
-    for (size_t q = 0; q < (size_t)n_e * n_f; ++q) W[C.o_cef + q] = 0.0;
+    for (size_t q = L0; q < (size_t)n_e * n_f; q += LS) W[C.o_cef + q] = 0.0;
+    T.sync();
     auto L = [&](int k, int lf, int ae, int m) -> double& {
       return W[C.o_lev + (size_t)(k % 3) * C.maxlevel + (size_t)lf * C.slab[k] + C.eoff[k * n_e + ae] + m];
     };
@@ -191,11 +222,12 @@ SC_HD double sc_schwarz(const BoysDev& B, const SClass& C, const Slice& W, const
         }
         const double pref = 2.0 * kPi * kPi * ::sqrt(kPi) / (p * q * ::sqrt(pq)) * W[ob + 1] * W[ok + 1];
         sc_boys(B, lt, t, fm);
-        for (int m = 0; m <= lt; ++m) L(0, 0, 0, m) = pref * fm[m];
+        for (int m = L0; m <= lt; m += LS) L(0, 0, 0, m) = pref * fm[m];
+        T.sync();
         const double inv2pq = 0.5 / pq, q_pq = q / pq, p_pq = p / pq;
         const double inv2p = W[ob + 4], inv2q = W[ok + 4];
-        for (int nd = 1; nd <= ne; ++nd)
-          for (int ti = 0; ti < sc_ncart(nd); ++ti) {
+        for (int nd = 1; nd <= ne; ++nd) {
+          for (int ti = L0; ti < sc_ncart(nd); ti += LS) {
             int x0, y0, z0;
             sc_triple(nd, ti, x0, y0, z0);
             const int i = sc_low_axis(x0, y0, z0);
@@ -211,9 +243,13 @@ SC_HD double sc_schwarz(const BoysDev& B, const SClass& C, const Slice& W, const
               L(0, 0, ad, m) = v;
             }
           }
-        for (int ae = 0; ae < n_e; ++ae) W[C.o_cef + (size_t)ae * n_f] += scale * L(0, 0, ae, 0);
+          T.sync();
+        }
+        for (int ae = L0; ae < n_e; ae += LS) W[C.o_cef + (size_t)ae * n_f] += scale * L(0, 0, ae, 0);
         for (int kd = 1; kd <= nf; ++kd) {
-          for (int fi = 0; fi < sc_ncart(kd); ++fi) {
+          const int nfk = sc_ncart(kd);
+          for (int idx = L0; idx < nfk * n_e; idx += LS) {
+            const int fi = idx / n_e, ea_ = idx - fi * n_e;
             int fx, fy, fz;
             sc_triple(kd, fi, fx, fy, fz);
             const int j = sc_low_axis(fx, fy, fz);
@@ -224,30 +260,30 @@ SC_HD double sc_schwarz(const BoysDev& B, const SClass& C, const Slice& W, const
             const double c2 = (double)(fj - 1) * inv2q;
             const int lf2 = two ? sc_within(gx - (j == 0), gy - (j == 1), gz - (j == 2)) : 0;
             const int lf = fi;
-            for (int nd = 0; nd <= ne; ++nd)
-              for (int ti = 0; ti < sc_ncart(nd); ++ti) {
-                int x0, y0, z0;
-                sc_triple(nd, ti, x0, y0, z0);
-                const int ea_ = sc_addr(x0, y0, z0);
-                const int ej = sc_get(x0, y0, z0, j);
-                const bool cross = ej >= 1;
-                const double cc = cross ? (double)ej * inv2pq : 0.0;
-                const int ax = cross ? sc_addr(x0 - (j == 0), y0 - (j == 1), z0 - (j == 2)) : 0;
-                for (int m = 0; m <= lt - nd - kd; ++m) {
-                  double v = kPA[j] * L(kd - 1, lf1, ea_, m) + wq[j] * L(kd - 1, lf1, ea_, m + 1);
-                  if (two) v += c2 * (L(kd - 2, lf2, ea_, m) - p_pq * L(kd - 2, lf2, ea_, m + 1));
-                  if (cross) v += cc * L(kd - 1, lf1, ax, m + 1);
-                  L(kd, lf, ea_, m) = v;
-                }
-              }
+            const int nd = sc_degree(ea_);
+            int x0, y0, z0;
+            sc_triple(nd, ea_ - sc_deg_below(nd), x0, y0, z0);
+            const int ej = sc_get(x0, y0, z0, j);
+            const bool cross = ej >= 1;
+            const double cc = cross ? (double)ej * inv2pq : 0.0;
+            const int ax = cross ? sc_addr(x0 - (j == 0), y0 - (j == 1), z0 - (j == 2)) : 0;
+            for (int m = 0; m <= lt - nd - kd; ++m) {
+              double v = kPA[j] * L(kd - 1, lf1, ea_, m) + wq[j] * L(kd - 1, lf1, ea_, m + 1);
+              if (two) v += c2 * (L(kd - 2, lf2, ea_, m) - p_pq * L(kd - 2, lf2, ea_, m + 1));
+              if (cross) v += cc * L(kd - 1, lf1, ax, m + 1);
+              L(kd, lf, ea_, m) = v;
+            }
           }
-          for (int fi = 0; fi < sc_ncart(kd); ++fi) {
+          T.sync();
+          for (int idx = L0; idx < nfk * n_e; idx += LS) {
+            const int fi = idx / n_e, ae = idx - fi * n_e;
             int fx, fy, fz;
             sc_triple(kd, fi, fx, fy, fz);
             const int af = sc_addr(fx, fy, fz);
-            for (int ae = 0; ae < n_e; ++ae) W[C.o_cef + (size_t)ae * n_f + af] += scale * L(kd, fi, ae, 0);
+            W[C.o_cef + (size_t)ae * n_f + af] += scale * L(kd, fi, ae, 0);
           }
         }
+        T.sync();
       }
     }
     // contracted HRR, bra then ket (src/engine/os_eri.rs:3040-3143)
@@ -256,70 +292,68 @@ SC_HD double sc_schwarz(const BoysDev& B, const SClass& C, const Slice& W, const
     const int nfr = n_f - fb;
     size_t prev = C.o_prev, cur = C.o_cur;
     for (int fg = fb; fg < n_f; ++fg) {
-      for (int dg = la; dg <= ne; ++dg)
-        for (int ti = 0; ti < sc_ncart(dg); ++ti) {
-          const int ae = sc_deg_below(dg) + ti;
-          W[prev + ae] = W[C.o_cef + (size_t)ae * n_f + fg];
-        }
+      for (int ae = fb + L0; ae < sc_deg_below(ne + 1); ae += LS) W[prev + ae] = W[C.o_cef + (size_t)ae * n_f + fg];
+      T.sync();
       for (int kb = 1; kb <= lb; ++kb) {
-        for (int bi = 0; bi < sc_ncart(kb); ++bi) {
+        const int cnt = sc_deg_below(ne - kb + 1) - fb;
+        for (int idx = L0; idx < sc_ncart(kb) * cnt; idx += LS) {
+          const int bi = idx / cnt, ae = fb + (idx - bi * cnt);
           int bx, by, bz;
           sc_triple(kb, bi, bx, by, bz);
           const int i = sc_low_axis(bx, by, bz);
           const int b1 = sc_within(bx - (i == 0), by - (i == 1), bz - (i == 2));
-          for (int dg = la; dg <= ne - kb; ++dg)
-            for (int ti = 0; ti < sc_ncart(dg); ++ti) {
-              int x0, y0, z0;
-              sc_triple(dg, ti, x0, y0, z0);
-              const int ae = sc_deg_below(dg) + ti;
-              const int a1 = sc_addr(x0 + (i == 0), y0 + (i == 1), z0 + (i == 2));
-              W[cur + (size_t)bi * n_e + ae] = W[prev + (size_t)b1 * n_e + a1] + ab[i] * W[prev + (size_t)b1 * n_e + ae];
-            }
+          const int dg = sc_degree(ae);
+          int x0, y0, z0;
+          sc_triple(dg, ae - sc_deg_below(dg), x0, y0, z0);
+          const int a1 = sc_addr(x0 + (i == 0), y0 + (i == 1), z0 + (i == 2));
+          W[cur + (size_t)bi * n_e + ae] = W[prev + (size_t)b1 * n_e + a1] + ab[i] * W[prev + (size_t)b1 * n_e + ae];
         }
+        T.sync();
         const size_t t = prev;
         prev = cur;
         cur = t;
       }
-      for (int bi = 0; bi < nb; ++bi)
-        for (int ai = 0; ai < na; ++ai)
-          W[C.o_bra + ((size_t)ai * nb + bi) * nfr + (fg - fb)] = W[prev + (size_t)bi * n_e + fb + ai];
+      for (int idx = L0; idx < nb * na; idx += LS) {
+        const int bi = idx / na, ai = idx - bi * na;
+        W[C.o_bra + ((size_t)ai * nb + bi) * nfr + (fg - fb)] = W[prev + (size_t)bi * n_e + fb + ai];
+      }
+      T.sync();
     }
     const int nc = na, ndd = nb;
-    size_t kprev = C.o_kprev, kcur = C.o_kcur;
     for (int ai = 0; ai < na; ++ai)
       for (int bi = 0; bi < nb; ++bi) {
         const size_t row = ((size_t)ai * nb + bi) * nfr;
-        size_t kp = kprev, kc = kcur;
-        for (int dg = la; dg <= nf; ++dg)
-          for (int ti = 0; ti < sc_ncart(dg); ++ti) {
-            const int ce = sc_deg_below(dg) + ti;
-            W[kp + ce] = W[C.o_bra + row + (ce - fb)];
-          }
+        size_t kp = C.o_kprev, kc = C.o_kcur;
+        for (int ce = fb + L0; ce < sc_deg_below(nf + 1); ce += LS) W[kp + ce] = W[C.o_bra + row + (ce - fb)];
+        T.sync();
         for (int kd = 1; kd <= lb; ++kd) {
-          for (int di = 0; di < sc_ncart(kd); ++di) {
+          const int cnt = sc_deg_below(nf - kd + 1) - fb;
+          for (int idx = L0; idx < sc_ncart(kd) * cnt; idx += LS) {
+            const int di = idx / cnt, ce = fb + (idx - di * cnt);
             int dx, dy, dz;
             sc_triple(kd, di, dx, dy, dz);
             const int j = sc_low_axis(dx, dy, dz);
             const int d1 = sc_within(dx - (j == 0), dy - (j == 1), dz - (j == 2));
-            for (int dg = la; dg <= nf - kd; ++dg)
-              for (int ti = 0; ti < sc_ncart(dg); ++ti) {
-                int x0, y0, z0;
-                sc_triple(dg, ti, x0, y0, z0);
-                const int ce = sc_deg_below(dg) + ti;
-                const int c1 = sc_addr(x0 + (j == 0), y0 + (j == 1), z0 + (j == 2));
-                W[kc + (size_t)di * n_f + ce] = W[kp + (size_t)d1 * n_f + c1] + ab[j] * W[kp + (size_t)d1 * n_f + ce];
-              }
+            const int dg = sc_degree(ce);
+            int x0, y0, z0;
+            sc_triple(dg, ce - sc_deg_below(dg), x0, y0, z0);
+            const int c1 = sc_addr(x0 + (j == 0), y0 + (j == 1), z0 + (j == 2));
+            W[kc + (size_t)di * n_f + ce] = W[kp + (size_t)d1 * n_f + c1] + ab[j] * W[kp + (size_t)d1 * n_f + ce];
           }
+          T.sync();
           const size_t t = kp;
           kp = kc;
           kc = t;
         }
-        for (int ci = 0; ci < nc; ++ci)
-          for (int di = 0; di < ndd; ++di)
-            W[C.o_blk + (((size_t)ai * nb + bi) * nc + ci) * ndd + di] += W[kp + (size_t)di * n_f + fb + ci];
+        for (int idx = L0; idx < nc * ndd; idx += LS) {
+          const int ci = idx / ndd, di = idx - ci * ndd;
+          W[C.o_blk + (((size_t)ai * nb + bi) * nc + ci) * ndd + di] += W[kp + (size_t)di * n_f + fb + ci];
+        }
+        T.sync();
       }
   }
-  // per-axis c2s (src/spherical.rs:121-179), then the diagonal maximum
+  // per-axis c2s (src/spherical.rs:121-179), then the diagonal maximum;
+  // every output element sums its inputs in the serial order from 0.0
   int dims[4] = {na, nb, na, nb};
   const double* mats[4] = {c2a, c2b, c2a, c2b};
   const int lsh[4] = {la, lb, la, lb};
@@ -330,18 +364,19 @@ SC_HD double sc_schwarz(const BoysDev& B, const SClass& C, const Slice& W, const
     size_t outer = 1, inner = 1;
     for (int q = 0; q < axis; ++q) outer *= dims[q];
     for (int q = axis + 1; q < 4; ++q) inner *= dims[q];
-    for (size_t q = 0; q < outer * n_o * inner; ++q) W[oth + q] = 0.0;
     const double* M = mats[axis];
-    for (size_t o = 0; o < outer; ++o)
-      for (int r = 0; r < n_o; ++r) {
-        const size_t dst = oth + (o * n_o + r) * inner;
-        for (int j = 0; j < n_in; ++j) {
-          const double m = M[(size_t)r * n_in + j];
-          if (m == 0.0) continue;
-          const size_t src = cur + (o * n_in + j) * inner;
-          for (size_t s2 = 0; s2 < inner; ++s2) W[dst + s2] += m * W[src + s2];
-        }
+    for (size_t idx = L0; idx < outer * n_o * inner; idx += LS) {
+      const size_t s2 = idx % inner, t = idx / inner;
+      const size_t r = t % n_o, o = t / n_o;
+      double v = 0.0;
+      for (int j = 0; j < n_in; ++j) {
+        const double m = M[r * n_in + j];
+        if (m == 0.0) continue;
+        v += m * W[cur + (o * n_in + j) * inner + s2];
       }
+      W[oth + idx] = v;
+    }
+    T.sync();
     dims[axis] = n_o;
     const size_t t = cur;
     cur = oth;
@@ -349,8 +384,15 @@ SC_HD double sc_schwarz(const BoysDev& B, const SClass& C, const Slice& W, const
   }
   const int ni = dims[0], nj = dims[1];
   double mx = 0.0;
-  for (int mu = 0; mu < ni; ++mu)
-    for (int nu = 0; nu < nj; ++nu) mx = fmax(mx, fabs(W[cur + (((size_t)mu * nj + nu) * ni + mu) * nj + nu]));
+  for (int idx = L0; idx < ni * nj; idx += LS) {
+    const int mu = idx / nj, nu = idx - mu * nj;
+    mx = fmax(mx, fabs(W[cur + (((size_t)mu * nj + nu) * ni + mu) * nj + nu]));
+  }
+#ifdef __CUDA_ARCH__
+  if (LS > 1)
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+#endif
+  T.sync();
   return ::sqrt(mx);
 }
 

@@ -25,8 +25,9 @@ struct SchwarzPairsDev {
   const long long* kappa_off;
   const double* kappa;
 };
-// q_out[x] = Q of listed pair x; the scratch holds grid * 128 * C.total doubles.
+// q_out[x] = Q of listed pair x, evaluated by teams of `team` lanes (1 or
+// 32); the scratch holds grid * (128 / team) * C.total doubles.
 cudaError_t launch_schwarz_exact(const sc::BoysDev& B, const sc::SClass& C, const SchwarzPairsDev& in,
-                                 double* scratch, int grid, double* q_out, cudaStream_t s);
+                                 double* scratch, int grid, int team, double* q_out, cudaStream_t s);
 
 }  // namespace igpu

@@ -88,15 +88,24 @@ def test_eri_builder_matches_dense():
     assert float(np.max(np.abs(O4[rows] - R4[rows]))) < 1e-13 * float(np.max(np.abs(ref)))
 
 
-@pytest.mark.parametrize("system", ["jk-8atom", "jk-64atom", "grad-100atom", "sph-f-6atom"])
+def g_molecule(natom, seed=5):
+    """The molecule-batch recipe (spherical s,s,p,p,d,f,g, 3 primitives)."""
+    rng = np.random.default_rng(seed)
+    centers = S.place_atoms(rng, natom, 2.5 * natom ** (1.0 / 3.0), 1.6)
+    return S.build_shells(rng, centers, "ssppdfg", 3, 0.1, 2.4, 0.2, 1.0, spherical=True)
+
+
+@pytest.mark.parametrize("system", ["jk-8atom", "jk-64atom", "grad-100atom", "sph-f-6atom", "g-3atom"])
 def test_schwarz_bounds_are_the_reference_bit_for_bit(system):
     """The plan screens with the reference's own Schwarz bounds, bit for bit
     (every pair of these contracted bases is an OS/HGP diagonal under the
-    Auto policy), so the screened quartet lists match by construction."""
+    Auto policy), so the screened quartet lists match by construction.  The
+    f and g cases run the warp-per-pair evaluation of the larger classes."""
     shells = {"jk-8atom": lambda: S.jk_system(natom=8, side=8.0)["shells"],
               "jk-64atom": lambda: S.jk_system()["shells"],
               "grad-100atom": lambda: S.grad_system()["shells"],
-              "sph-f-6atom": lambda: S.jk_spherical_system(natom=6, side=9.0)["shells"]}[system]()
+              "sph-f-6atom": lambda: S.jk_spherical_system(natom=6, side=9.0)["shells"],
+              "g-3atom": lambda: g_molecule(3)}[system]()
     q = ib.Basis(shells).schwarz_bounds().reshape(len(shells), -1)
     qo = O.OracleBasis(shells).schwarz()
     assert q.view(np.uint64).tolist() == qo.view(np.uint64).tolist()

@@ -58,6 +58,13 @@ def assert_bitwise(shells):
     return int(rys.sum())
 
 
+def g_molecule(natom, seed=5):
+    """The molecule-batch recipe (spherical s,s,p,p,d,f,g, 3 primitives)."""
+    rng = np.random.default_rng(seed)
+    centers = S.place_atoms(rng, natom, 2.5 * natom ** (1.0 / 3.0), 1.6)
+    return S.build_shells(rng, centers, "ssppdfg", 3, 0.1, 2.4, 0.2, 1.0, spherical=True)
+
+
 CASES = {
     "dense-6atom": lambda: S.dense_eri_system()["shells"],
     "jk-fixture-cart": lambda: S.direct_contractor_fixture(False),
@@ -65,6 +72,7 @@ CASES = {
     "grad-fixture-cart": lambda: S.direct_grad_fixture(False),
     "grad-fixture-sph": lambda: S.direct_grad_fixture(True),
     "sph-f-6atom": lambda: S.jk_spherical_system(natom=6, side=9.0)["shells"],
+    "g-3atom": lambda: g_molecule(3),
 }
 
 
