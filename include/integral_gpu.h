@@ -149,7 +149,7 @@ int igpu_schwarz(const igpu_plan* plan, double* q);
  * NaN and it is counted in *n_rys (n_rys may be NULL).  A plan holds the
  * device evaluation for those pairs (within 1e-14 of the reference). */
 int igpu_schwarz_bounds(const igpu_shell* shells, size_t nsh, double* q, size_t* n_rys);
-/* Plan cutoff for IGPU_PRECISION_MIXED (default 1e-4). */
+/* Plan cutoff for IGPU_PRECISION_MIXED (default 1e-3). */
 int igpu_set_mixed_cutoff(igpu_plan* plan, double cutoff);
 /* Primitive screen of the FP32 quartets of IGPU_PRECISION_MIXED J/K (no
  * counterpart in the reference, which evaluates every primitive quartet that

@@ -805,7 +805,7 @@ class DirectContractor:
 
     def set_mixed_cutoff(self, cutoff: float):
         """MIXED precision: quartets with Q_bra*Q_ket*max|D| below `cutoff`
-        (default 1e-4) run in FP32 (igpu_set_mixed_cutoff)."""
+        (default 1e-3) run in FP32 (igpu_set_mixed_cutoff)."""
         _lib.check(_lib.lib().igpu_set_mixed_cutoff(self._plan.h, float(cutoff)))
 
     def mixed_cutoffs(self):

@@ -272,6 +272,7 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   CK(cudaStreamIsCapturing(s, &cap));
   const bool capturing = cap == cudaStreamCaptureStatusActive;
+  const double prim_cut0 = A.prim_cut;
   for (size_t li = 0; li < nl; ++li) {
     Launch* L = ts.launches[li].get();
     if (L->total == 0) continue;
@@ -305,6 +306,7 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     A.task.nbra = L->nbra;
     A.task.total = L->total;
     A.fp32 = L->fp32 ? 1 : 0;
+    A.prim_cut = prim_cut0 / fp32_class_scale(class_lmax(L->pcb, L->pck));
     A.builder_swap = L->builder_swap;
     // under stream capture the records are external nodes, so that the
     // graph records them on every replay (the flag is only valid there)
@@ -401,6 +403,21 @@ std::unique_ptr<Launch> make_launch(igpu_plan* P, int pcb, int pck, bool fp32, c
   return L;
 }
 
+// How much smaller a class's FP32 cutoffs are than the plan's, by the
+// largest angular momentum of its four shells: the recurrences' cancellation
+// amplifies FP32 rounding more at high l, and on spread molecules with f and
+// g shells the mixed energy error per unit of cutoff grew about 100-fold per
+// unit of l above 2.  So f classes take a quartet into FP32 below 1/100 of
+// the cutoff (and skip primitive quartets below 1/100 of the primitive
+// cutoff), g classes below 1/10^4.
+double fp32_class_scale(int lmax) { return lmax <= 2 ? 1.0 : std::pow(100.0, lmax - 2); }
+
+int class_lmax(int pca, int pcb) {
+  const int a = pc_la_host(pca), b = pca - a * (a + 1) / 2;
+  const int c = pc_la_host(pcb), d = pcb - c * (c + 1) / 2;
+  return std::max(std::max(a, b), std::max(c, d));
+}
+
 // Screened J/K task lists for threshold tau: for every class pair (CA >= CB)
 // and bra of CA, the kets of CB with Q_bra*Q_ket >= tau (a prefix of the
 // Q-sorted list; the upper triangle when CA == CB).  With fp64_cut > 0 the
@@ -413,6 +430,8 @@ int build_jk_tasks(igpu_plan* P, double tau, double fp64_cut, TaskSet& ts) {
       const auto& B = P->class_pairs[ca];
       const auto& K = P->class_pairs[cb];
       if (B.empty() || K.empty()) continue;
+      // the class's own FP32 cutoff (fp32_class_scale)
+      const double cut_c = fp64_cut / fp32_class_scale(class_lmax(ca, cb));
       std::vector<double> qk(K.size());
       for (size_t x = 0; x < K.size(); ++x) qk[x] = P->pairs[K[x]].q;
       // One segment per (bra, ket group of equal primitive-pair count): the
@@ -448,7 +467,7 @@ int build_jk_tasks(igpu_plan* P, double tau, double fp64_cut, TaskSet& ts) {
             size_t l2 = gs, h2 = end;
             while (l2 < h2) {
               size_t mid = (l2 + h2) / 2;
-              if (qb * qk[mid] >= fp64_cut)
+              if (qb * qk[mid] >= cut_c)
                 l2 = mid + 1;
               else
                 h2 = mid;

@@ -176,7 +176,7 @@ struct igpu_plan {
   std::map<int, int> tuned_bps;
   int tune_bps = 0;
   std::unique_ptr<TaskSet> dense_tasks;
-  double mixed_cutoff = 1e-4;
+  double mixed_cutoff = 1e-3;
   // primitive screen of the FP32 launches of the mixed path: bound * max|D|
   // below this skips a primitive quartet (0: none)
   double mixed_prim_cut = 1e-15;
@@ -215,6 +215,8 @@ double model_flops_quartet(int la, int lb, int lc, int ld, bool sph, int ndens, 
 double model_flops_grad_prim(int la, int lb, int lc, int ld);
 double model_flops_grad_quartet(int la, int lb, int lc, int ld, bool sph, int nterm_c, int nterm_x);
 double mixed_split(double cutoff, double dmax);
+double fp32_class_scale(int lmax);
+int class_lmax(int pca, int pcb);
 int tune_key(int pcb, int pck, bool fp32, bool grad);
 void tune_record(igpu_plan* P, int m, bool grad, std::map<int, std::map<int, float>>& best);
 void tune_keep(igpu_plan* P, const std::map<int, std::map<int, float>>& best, bool bps);

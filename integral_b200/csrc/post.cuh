@@ -1009,10 +1009,13 @@ __device__ __forceinline__ void team_c2s_axis(const X* in, X* out, const X* M, i
 }
 
 // Shared-memory copies of the four c2s matrices of a class (l_a, l_b, l_c,
-// l_d), rows of at most 7 x 10.
-constexpr int C2S_TILE = 70;
+// l_d), each (2l+1) x n_cart, at most 9 x 15 (g shells).
+constexpr int C2S_TILE = 9 * 15;
 template <int LA, int LB, int LC, int LD, typename X>
 __device__ __forceinline__ void stage_c2s(const KernelArgs& A, X* s_m) {
+  static_assert((2 * LA + 1) * ncart(LA) <= C2S_TILE && (2 * LB + 1) * ncart(LB) <= C2S_TILE &&
+                    (2 * LC + 1) * ncart(LC) <= C2S_TILE && (2 * LD + 1) * ncart(LD) <= C2S_TILE,
+                "c2s matrix larger than its shared-memory tile");
   const int ls[4] = {LA, LB, LC, LD};
   for (int t = threadIdx.x; t < 4 * C2S_TILE; t += blockDim.x) {
     const int ax = t / C2S_TILE, i = t - ax * C2S_TILE;

@@ -88,3 +88,31 @@ def test_gradient_with_g_shells():
     assert st["quartets"] == cnt and st["quartet_hash"] == hsh
     assert float(np.max(np.abs(out - ref))) < 1e-10 * float(np.max(np.abs(ref)))
     assert float(np.max(np.abs(out.sum(axis=0)))) < 1e-9 * float(np.max(np.abs(out)))
+
+
+def spread_molecule(natom, letters, seed=9):
+    """Atoms over a 12-bohr cube with exponents 0.3*2.4^k: the shell pairs
+    span up to 10 bohr, where FP32 rounding in the recurrences of high-l
+    classes is amplified most."""
+    rng = np.random.default_rng(seed)
+    centers = S.place_atoms(rng, natom, 12.0, 1.8)
+    shells = S.build_shells(rng, centers, letters, 3, 0.3, 2.4, 0.2, 1.0, spherical=True)
+    nao = S.nao_of(shells)
+    return shells, S.densities(rng, nao, max(1, nao // 4), 1)
+
+
+@pytest.mark.parametrize("letters", ["ssppdf", "ssppdfg"], ids=["f", "g"])
+def test_mixed_precision_error_with_high_l(letters):
+    """MIXED precision at the default cutoffs keeps the energy error of f and
+    g systems within 1e-7 Eh: classes with f or g shells take quartets into
+    FP32 only below 1/100 or 1/10^4 of the cutoff (at one cutoff for all
+    classes this 9-atom g system was off by 2.8e-4 Eh at 1e-3)."""
+    shells, D = spread_molecule(9, letters)
+    dc = ib.Basis(shells).direct_contractor()
+    J64, K64 = dc.jk(D, 1e-11, precision=0)
+    J32, K32 = dc.jk(D, 1e-11, precision=1)
+    st = dc.last_stats()
+    assert st["quartets_fp32"] > 0.3 * st["quartets"]
+    e = lambda Jx, Kx: 0.5 * float(np.sum(D[0] * (Jx[0] - 0.5 * Kx[0])))
+    assert abs(e(J32, K32) - e(J64, K64)) < 1e-7
+
