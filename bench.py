@@ -54,7 +54,7 @@ UNIT = "quartets/s"
 # dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch of
 # this workload's kernels, from a one-pass ncu capture on a B200
 # (profiles/quartet_kernel_2120_fp32_traffic.md); bytes per launch.
-NCU_TRAFFIC = {"quartet_kernel(21|20) fp32": 612.62e6 + 526.42e6}
+NCU_TRAFFIC = {"quartet_kernel(21|20) fp32": 68.02e6 + 70.12e6}
 
 
 def parse():
@@ -75,6 +75,10 @@ def parse():
     # a stride > 1 still decodes every task (the subset is a filter), so its
     # quartets/s understates the full build's
     p.add_argument("--grad-stride", type=int, default=1)
+    p.add_argument("--batch-molecules", type=int, default=256,
+                   help="batch workload: time a seeded subset of this many of the 256 molecules")
+    p.add_argument("--batch-gradient", type=int, default=1,
+                   help="batch workload: 1 adds the density-direct gradient to every step, 0 J/K only")
     p.add_argument("--mixed-cutoff", type=float, default=None,
                    help="Schwarz-product cutoff below which quartets run in FP32 (default: the library's)")
     p.add_argument("--profile-case", action="store_true",
@@ -375,6 +379,10 @@ def batch_bench(args):
 
     sysb = S.molecule_batch()
     mols = sysb["molecules"]
+    nfull = len(mols)
+    if args.batch_molecules < nfull:
+        keep = np.sort(np.random.default_rng(23).choice(nfull, args.batch_molecules, replace=False))
+        mols = [mols[k] for k in keep]
     thr = 1e-11
     t0 = time.perf_counter()
     batch = ib.MoleculeBatch([m["shells"] for m in mols])
@@ -383,12 +391,13 @@ def batch_bench(args):
         batch.set_mixed_cutoff(args.mixed_cutoff)
     dens = [m["dens"] for m in mols]
     want_grad = False
-    try:
-        batch.jk_grad(dens, thr, precision=0, gradient=True)
-        want_grad = True
-    except ib.IntegralError as e:
-        if e.code != -11:
-            raise
+    if args.batch_gradient:
+        try:
+            batch.jk_grad(dens, thr, precision=0, gradient=True)
+            want_grad = True
+        except ib.IntegralError as e:
+            if e.code != -11:
+                raise
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float64, device="cuda")
 
     def timed(prec):
@@ -419,23 +428,26 @@ def batch_bench(args):
     steps = args.steps
     h2d = int(8 * sum(D.size for D in dens))
     natoms = int(sum(batch.natom(m) for m in range(nmol)))
-    # CPU baseline: the oracle's J/K on every host thread over seeded bra
-    # samples of a seeded sample of molecules; its screened quartets per
-    # second over the batch's mean quartets per molecule give molecules/s
+    # CPU baseline: the oracle's J/K on every host thread; its screened
+    # quartets per second over the batch's mean quartets per molecule give
+    # molecules/s
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_py as O
     nthreads = os.cpu_count() or 1
-    rng = np.random.default_rng(17)
-    pick = rng.choice(nmol, 4, replace=False)
+    # (a g shell's OS/HGP quartets cost the oracle up to a tenth of a second
+    # each, so the sample is the whole J/K of the batch's smallest molecules,
+    # taken until 15 s of host time)
+    pick = []
     cpu_q, cpu_s = 0, 0.0
-    for k in pick:
+    for k in np.argsort([batch.natom(m) for m in range(nmol)], kind="stable"):
+        if cpu_s > 15.0:
+            break
         ob = O.OracleBasis(mols[k]["shells"])
-        nsh = len(mols[k]["shells"])
-        bras = rng.choice(nsh * (nsh + 1) // 2, min(2 * nthreads, nsh * (nsh + 1) // 2), replace=False)
         t0 = time.perf_counter()
-        _, _, c, _ = ob.direct_jk(dens[k][None], thr, bras=bras, nthreads=nthreads)
+        _, _, c, _ = ob.direct_jk(dens[k][None], thr, nthreads=nthreads)
         cpu_s += time.perf_counter() - t0
         cpu_q += c
+        pick.append(int(k))
     # the J/K quartets of one step (the GPU step also counts the gradient's)
     batch.jk_grad(dens, thr, precision=0, gradient=False)
     q_per_mol = batch.last_stats()["quartets"] / nmol
@@ -445,9 +457,10 @@ def batch_bench(args):
         "warmup": args.warmup, "ms_per_step": ms32 / steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "fp32-mixed (fp64 accumulation)",
         "data": "synthetic (seeded generator, no data set)",
-        "config": {"workload": "256 molecules, 4..40 atoms, s,s,p,p,d,f,g spherical, 3 primitives, one density "
+        "config": {"workload": "%d molecules (%s), 4..40 atoms, s,s,p,p,d,f,g spherical, 3 primitives, one density "
                                "each (nocc = nao/4), tau 1e-11, one CUDA graph per step%s"
-                               % ("" if want_grad else "; J/K only (gradient classes of g shells not compiled)"),
+                               % (nmol, "all 256" if nmol == nfull else "a seeded subset of the 256",
+                                  "" if want_grad else "; J/K only"),
                    "molecules": nmol, "atoms": natoms,
                    "nao_total": int(sum(batch.nao(m) for m in range(nmol))), "quartets_per_step": q32 // steps,
                    "batch_setup_s": setup_s, "l2": "flushed between steps (512 MB write)",
@@ -462,10 +475,10 @@ def batch_bench(args):
         "gpu_launches": l32,
         "cpu_baseline": {"value": cpu_q / cpu_s / q_per_mol, "unit": "molecules/s", "cores": nthreads,
                          "kind": "port",
-                         "sample": "J/K of %d seeded bra pairs in each of %d seeded molecules (%s atoms; %d screened "
+                         "sample": "whole J/K of the %d smallest molecules of the batch (%s atoms; %d screened "
                                    "quartets, %.1f s), all threads, over the batch's mean %.0f J/K quartets per "
                                    "molecule: J/K only%s; %s"
-                                   % (2 * nthreads, len(pick), ",".join(str(batch.natom(int(k))) for k in pick), cpu_q,
+                                   % (len(pick), ",".join(str(batch.natom(k)) for k in pick), cpu_q,
                                       cpu_s, q_per_mol, " (the GPU step adds the gradient)" if want_grad else "",
                                       CPU_KIND)},
     }
