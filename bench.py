@@ -387,6 +387,7 @@ def batch_bench(args):
     t0 = time.perf_counter()
     batch = ib.MoleculeBatch([m["shells"] for m in mols])
     setup_s = time.perf_counter() - t0
+    print("batch of %d molecules set up in %.1f s" % (len(mols), setup_s), file=sys.stderr, flush=True)
     if args.mixed_cutoff is not None:
         batch.set_mixed_cutoff(args.mixed_cutoff)
     dens = [m["dens"] for m in mols]
@@ -404,6 +405,7 @@ def batch_bench(args):
         for _ in range(args.warmup):
             batch.jk_grad(dens, thr, precision=prec, gradient=want_grad)
         ms, wall, q, launches, out = 0.0, 0.0, 0, 0, None
+        print("precision %d: warm-up done" % prec, file=sys.stderr, flush=True)
         for _ in range(args.steps):
             flush.fill_(1.0)
             torch.cuda.synchronize()
@@ -448,9 +450,13 @@ def batch_bench(args):
         cpu_s += time.perf_counter() - t0
         cpu_q += c
         pick.append(int(k))
-    # the J/K quartets of one step (the GPU step also counts the gradient's)
-    batch.jk_grad(dens, thr, precision=0, gradient=False)
-    q_per_mol = batch.last_stats()["quartets"] / nmol
+    # the J/K quartets of one step (a step with the gradient also counts the
+    # gradient's)
+    if want_grad:
+        batch.jk_grad(dens, thr, precision=0, gradient=False)
+        q_per_mol = batch.last_stats()["quartets"] / nmol
+    else:
+        q_per_mol = q64 / args.steps / nmol
     line = {
         "metric": "molecule batch J/K%s molecules/s (FP32-mixed) on B200" % (" + gradient" if want_grad else ""),
         "unit": "molecules/s", "value": nmol * steps / (ms32 * 1e-3), "n_gpus": 1, "steps": steps,
