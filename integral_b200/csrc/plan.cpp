@@ -290,7 +290,14 @@ int run_tasks(igpu_plan* P, TaskSet& ts, KernelArgs A, cudaStream_t s, uint32_t&
     A.slot_doubles = slot_with_acc(e, L->pcb, A);
     A.acc_offset = e->slot;
     A.work_counter = lg.work.p + li;
-    int mult = 16;
+    // tasks a warp claims per grab: (32 / team) x mult.  Untuned, mult is 16,
+    // or less when the launch has so few tasks that 16 would leave warps of
+    // the grid without work: every warp should find at least four grabs,
+    // which matters for classes of few, heavy quartets (g shells, small
+    // molecules)
+    const unsigned long long warps = (unsigned long long)grid * 4;
+    const unsigned long long fill = L->total / (4 * warps * (unsigned long long)(32 / e->team));
+    int mult = (int)std::max<unsigned long long>(1, std::min<unsigned long long>(16, fill));
     if (P->tune_mult) {
       mult = P->tune_mult;
     } else if (A.mode == MODE_JK || A.mode == MODE_GRAD) {

@@ -26,7 +26,9 @@ def test_autotune_keeps_results_and_sets_candidate_chunks():
     for r in prof:
         teams_per_warp = 32 // r["team"]
         assert r["chunk"] % teams_per_warp == 0 and r["chunk"] // teams_per_warp in (4, 8, 16, 32, 64)
-    assert all(c // (32 // r["team"]) == 16 for c, r in zip(before, prof))
+    # untuned: 16 grabs per warp-team set, fewer for launches too small to
+    # give every warp of the grid four grabs
+    assert all(1 <= c // (32 // r["team"]) <= 16 for c, r in zip(before, prof))
     for a, b in ((J0, J1), (K0, K1)):
         a, b = a.cpu().numpy(), b.cpu().numpy()
         assert float(np.max(np.abs(a - b))) < 1e-12 * float(np.max(np.abs(a)))
