@@ -127,7 +127,7 @@ __device__ __forceinline__ void accumulate_thread(const KernelArgs& A, const R* 
       }
       R x[NR], w[NR];
       if constexpr (sizeof(R) == 4) {
-        // FP32 launch: high l and T just below the asymptotic crossover take
+        // FP32 launch: quadratures of five or more roots (high l) take
         // FP64 roots and weights
         if (roots_in_fp64<NR, R>(h.T)) {
           const double T64 = quartet_T64(A.prims[pb.prim_off + ip], A.prims[pk.prim_off + kq], A.omega);
@@ -253,7 +253,7 @@ __device__ __forceinline__ void team_pass(const KernelArgs& A, const R* s_tab, c
         h = quartet_header_f(A.primsf[pb.prim_off + ip], A.primsf[pk.prim_off + kq], acx, acy, acz, A.omega);
       else
         h = quartet_header<R>(A.prims[pb.prim_off + ip], A.prims[pk.prim_off + kq], A.omega);
-      // FP32 launch: high l and T just below the asymptotic crossover take
+      // FP32 launch: quadratures of five or more roots (high l) take
       // FP64 roots and weights
       const bool r64 = roots_in_fp64<NR, R>(h.T);
       const double T64 = r64 ? quartet_T64(A.prims[pb.prim_off + ip], A.prims[pk.prim_off + kq], A.omega) : 0.0;
