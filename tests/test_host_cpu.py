@@ -270,3 +270,15 @@ def test_bench_reference_arm_prints_the_contract_line():
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_integration_guide_binds_every_entry_point():
+    """The Rust extern block of the integration guide declares every entry
+    point of the header, and nothing else."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    header = open(os.path.join(root, "include", "integral_gpu.h")).read()
+    guide = open(os.path.join(root, "INTEGRATION.md")).read()
+    declared = set(re.findall(r"\b(igpu_[a-z0-9_]+)\s*\(", header))
+    bound = set(re.findall(r"pub fn (igpu_[a-z0-9_]+)", guide))
+    assert declared == bound, (sorted(declared - bound), sorted(bound - declared))
+
