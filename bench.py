@@ -76,7 +76,8 @@ def parse():
     # quartets/s understates the full build's
     p.add_argument("--grad-stride", type=int, default=1)
     p.add_argument("--batch-molecules", type=int, default=256,
-                   help="batch workload: time a seeded subset of this many of the 256 molecules")
+                   help="batch workload: time a seeded subset of this many of the 256 molecules (the full "
+                        "batch is about 4.8e10 g-heavy quartets per step: hours on one GPU)")
     p.add_argument("--batch-gradient", type=int, default=1,
                    help="batch workload: 1 adds the density-direct gradient to every step, 0 J/K only")
     p.add_argument("--mixed-cutoff", type=float, default=None,
